@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Benchmark: RK4 particle-steps/s of the FTLE engine on B200.
+
+Workload (default, one FTLE window per step): 3D time-periodic ABC flow
+(A = sqrt3 + 0.1 sin t, B = sqrt2, C = 1) on a periodic 128^3 grid over
+[0, 2pi)^3, 64 snapshots over one period (time-periodic), 256^3 centroids x 6
+neighbours at delta = 1e-3 (100.7M particles), RK4 with h = 0.02 over T = 8
+(400 steps), time-blended snapshots.  Particle-steps = 6*N neighbours x steps.
+
+Legs (rank 0 prints one JSON line):
+  value     the chosen path (FP16 snapshots, FP32 split-representation
+            advection, FP64 Cauchy-Green) with inputs resident in HBM;
+  plain     the plain FP64 path on a slice of the same groups (the metric's
+            "vs plain FP64"), plus the chosen path's FTLE error against it;
+  e2e       the same window through the public API (FTLESolver.run) from
+            pinned host buffers: H2D of snapshots + positions, packing, the
+            window, D2H of the FTLE field, all inside the timed region;
+  cpu       the reference's CPU path (oracle/_ref ginterp + its RK4 loop) on
+            a bounded sample, on the host cores (rank 0, N = 1 only).
+
+``--impl reference`` times only the reference's CPU path (rank 0; other
+ranks exit 0).  Multi-GPU: one process per GPU (torchrun), each rank runs its
+own window (start time offset by rank) -- weak scaling, no collective on the
+data path; timing is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "RK4 particle-steps/s; chosen vs plain FP64 on 1 B200 at FTLE rel.err <=1e-3"
+UNIT = "particle-steps/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=["fp16", "bf16", "fp64"], default="fp16")
+    p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--snapshots", type=int, default=64)
+    p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
+    p.add_argument("--h", type=float, default=0.02)
+    p.add_argument("--T", type=float, default=8.0)
+    p.add_argument("--plain-fraction", type=float, default=0.125,
+                   help="share of the groups the plain FP64 leg advects")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-clocks", action="store_true")
+    return p.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# workload
+# ----------------------------------------------------------------------------
+
+def workload(args):
+    from pyftle_b200 import flows
+
+    L = 2.0 * math.pi
+    n = args.grid
+    ax = flows.periodic_axis(n, L)
+    S = args.snapshots
+    snap_dt = L / S
+    times = np.arange(S) * snap_dt
+    num_steps = int(round(args.T / args.h))
+    return dict(n=n, ax=ax, S=S, snap_dt=snap_dt, times=times, num_steps=num_steps, L=L,
+                seeds=args.seeds, delta=1e-3, h=args.h)
+
+
+def make_seeds(w, rank=0):
+    from pyftle_b200 import flows
+
+    m = w["seeds"]
+    c = (np.arange(m) + 0.5) * (w["L"] / m)
+    X, Y, Z = np.meshgrid(c, c, c)
+    cents = np.column_stack((X.ravel(), Y.ravel(), Z.ravel()))
+    del X, Y, Z
+    return flows.seeds_3d(cents, w["delta"])
+
+
+def workload_name(w):
+    return (f"ABC 3D periodic {w['n']}^3 grid, {w['S']} snapshots/period (blend), "
+            f"{w['seeds']}^3 centroids x 6 neighbours (delta 1e-3), RK4 h={w['h']} "
+            f"x {w['num_steps']} steps")
+
+
+# ----------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------
+
+CLOCK_Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    def __init__(self, device_index: int, enabled: bool = True):
+        self.proc = None
+        self.path = None
+        self.id = None
+        if not enabled:
+            return
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(device_index)
+            self.id = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        except Exception:
+            self.id = None
+        out_dir = os.path.join(REPO, "gpurun_out")
+        os.makedirs(out_dir, exist_ok=True)
+        self.path = os.path.join(out_dir, f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        if self.path is None:
+            return
+        cmd = ["nvidia-smi", f"--query-gpu={CLOCK_Q}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.id:
+            cmd[1:1] = ["-i", self.id]
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# reference arm / cpu baseline
+# ----------------------------------------------------------------------------
+
+def cpu_reference(w, steps=4, groups=32768, workers=None):
+    """The reference's CPU path (HOLD RK4, its ginterp) on a bounded sample."""
+    from oracle import ref_driver
+    from pyftle_b200 import flows
+
+    ax = w["ax"]
+    snaps = flows.abc_snapshots(ax, ax, ax, w["times"][:steps])
+    pts = flows.grid_points_3d(ax, ax, ax)
+    rng = np.random.default_rng(7)
+    cents = rng.uniform(0.0, w["L"], (groups, 3))
+    pos = flows.seeds_3d(cents, w["delta"])
+    r = ref_driver.time_reference(snaps, pts, (w["n"],) * 3, pos, w["snap_dt"], workers=workers)
+    r["sample"] = (f"{groups} random groups x 6 neighbours x {steps} RK4 HOLD steps per worker "
+                   f"on the {w['n']}^3 ABC snapshots, {r['cores']} worker(s)")
+    return r
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = workload(args)
+    for _ in range(max(1, min(args.warmup, 1))):
+        cpu_reference(w, steps=2, groups=4096)
+    vals = []
+    last = None
+    for _ in range(args.steps):
+        last = cpu_reference(w)
+        vals.append(last["value"])
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * last["seconds"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(w), "sample": last["sample"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": last["cores"],
+                         "kind": last["kind"], "sample": last["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from pyftle_b200 import (BlendedSnapshotSource, EngineOptions, FTLESolver,
+                             SnapshotSeries, create_integrator, create_interpolator, flows,
+                             run_window)
+    from pyftle_b200.interpolate import GridSpec
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = workload(args)
+    n = w["n"]
+    ax = w["ax"]
+    # rank r integrates its own window: start time offset by r snapshots (weak scaling)
+    t0 = rank * w["snap_dt"]
+    snaps_h = flows.abc_snapshots(ax, ax, ax, w["times"])
+    pts = flows.grid_points_3d(ax, ax, ax)
+    pos_h = make_seeds(w)
+    grid = GridSpec.from_points(pts, (n, n, n), periodic=True)
+    K = 6
+    N = pos_h.shape[0] // K
+    particle_steps = K * N * w["num_steps"]
+    dev = torch.device("cuda", local)
+
+    snaps_d = torch.from_numpy(snaps_h).to(dev)
+    pos0 = torch.from_numpy(pos_h).to(dev)
+    pos = torch.empty_like(pos0)
+    ftle = torch.empty(N, dtype=torch.float64, device=dev)
+    series = SnapshotSeries(grid, snaps_d, precision=args.precision, periodic_time=True)
+    kw = dict(integrator="rk4", time_mode="blend", h=w["h"], num_steps=w["num_steps"],
+              map_period=w["num_steps"] * w["h"], t0=t0, snapshot_dt=w["snap_dt"])
+    stream = torch.cuda.current_stream()
+
+    def one_window(out=None):
+        pos.copy_(pos0)
+        return run_window(series, pos, ftle_out=ftle if out is None else out, **kw)
+
+    for _ in range(args.warmup):
+        one_window()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local, enabled=not args.no_clocks)
+    clocks.start()
+    ev_start = torch.cuda.Event(enable_timing=True)
+    ev_end = torch.cuda.Event(enable_timing=True)
+    k_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    k_end = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev_start.record(stream)
+    for k in range(args.steps):
+        pos.copy_(pos0)
+        k_start[k].record(stream)
+        run_window(series, pos, ftle_out=ftle, **kw)
+        k_end[k].record(stream)
+    ev_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed_ms = max_over_ranks(ev_start.elapsed_time(ev_end))
+    kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in zip(k_start, k_end)]))
+    value = world * particle_steps * args.steps / (elapsed_ms / 1e3)
+    ftle_chosen = ftle.clone()
+
+    # --- plain FP64 leg (same groups, a slice of them) + FTLE error ----------
+    plain = None
+    if not args.no_plain and args.precision != "fp64":
+        m = max(1, int(N * args.plain_fraction))
+        sel = torch.cat([pos0[r * N:r * N + m] for r in range(K)]).contiguous()
+        series64 = SnapshotSeries(grid, snaps_d, precision="fp64", periodic_time=True)
+        f64 = torch.empty(m, dtype=torch.float64, device=dev)
+        p64 = sel.clone()
+        run_window(series64, p64, ftle_out=f64, **kw)  # warm-up
+        p64.copy_(sel)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        run_window(series64, p64, ftle_out=f64, **kw)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms64 = a.elapsed_time(b)
+        ref = f64
+        got = ftle_chosen[:m]
+        diff = (got - ref)
+        rel_l2 = float(torch.linalg.vector_norm(diff) / torch.linalg.vector_norm(ref))
+        rel_pt = (diff.abs() / ref.abs().clamp_min(1e-3))
+        plain = {
+            "value": K * m * w["num_steps"] / (ms64 / 1e3), "unit": UNIT,
+            "groups": m, "ms_per_window": ms64,
+            "speedup_chosen_vs_plain": None,
+            "ftle_rel_err_l2": rel_l2,
+            "ftle_abs_err_max": float(diff.abs().max()),
+            "ftle_rel_err_p99": float(torch.quantile(rel_pt[:min(m, 1 << 24)].float(), 0.99)),
+        }
+        plain["speedup_chosen_vs_plain"] = (value / world) / plain["value"]
+        del series64, p64, f64, sel
+    del snaps_d
+    torch.cuda.empty_cache()
+
+    # --- e2e: public API from pinned host buffers ----------------------------
+    e2e = None
+    if not args.no_e2e:
+        snaps_pin = torch.from_numpy(snaps_h).pin_memory()
+        pos_pin = torch.from_numpy(pos_h).pin_memory()
+        h2d = snaps_pin.numel() * 8 + pos_pin.numel() * 8
+        d2h = N * 8
+        integ = create_integrator("rk4", create_interpolator("grid", (n, n, n), periodic=True))
+        opts = EngineOptions(precision=args.precision)
+
+        def e2e_step():
+            src = BlendedSnapshotSource(snaps_pin, pts, pos_pin, (n, n, n), h=w["h"],
+                                        num_steps=w["num_steps"], snapshot_dt=w["snap_dt"],
+                                        t0=t0, periodic_space=True, periodic_time=True)
+            return FTLESolver(src, integ, options=opts).run()
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e_steps = max(1, min(args.steps, 2))
+        a.record(stream)
+        for _ in range(e_steps):
+            field = e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e_ms = max_over_ranks(a.elapsed_time(b))
+        e2e = {"value": world * particle_steps * e_steps / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e_ms / e_steps, "steps": e_steps,
+               "path": "FTLESolver.run(BlendedSnapshotSource(pinned host arrays))"}
+        assert np.isfinite(field).all()
+        del snaps_pin, pos_pin
+
+    # --- roofline of the dominant kernel --------------------------------------
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        peak = float(peaks["hbm_gbs"])
+        peak_src = "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    elem = 2 if args.precision in ("fp16", "bf16") else 8
+    bytes_per_ps = 4 * 8 * 3 * 2 * elem  # stages x corners x comps x snapshots x elem
+    achieved = bytes_per_ps * particle_steps / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(REPO, "profiles", "window_traffic.json")))
+        traffic = prof.get(args.precision)
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_src,
+                "algorithmic_bytes_per_particle_step": bytes_per_ps,
+                "kernel": "window_mixed_kernel" if elem == 2 else "window_f64_kernel",
+                "kernel_ms": kernel_ms}
+
+    # --- CPU baseline (rank 0, N = 1) ----------------------------------------
+    cpu = None
+    if not args.no_cpu and world == 1 and rank == 0:
+        r = cpu_reference(w)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+               "sample": r["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if elem == 2 else "f64", "data": "synthetic",
+            "config": {"workload": workload_name(w), "precision": args.precision,
+                       "particles": K * N, "groups": N, "rk4_steps": w["num_steps"],
+                       "particle_steps_per_window": particle_steps,
+                       "l2": "inputs larger than L2 (positions 2.4 GB, packed snapshots)",
+                       "rank_windows": "rank r starts at t0 = r * snapshot_dt"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": args.steps, "clocks": clk, "plain_fp64": plain,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

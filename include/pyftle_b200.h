@@ -1,0 +1,168 @@
+/*
+ * pyftle_b200.h -- C ABI of the B200 (sm_100a) FTLE engine.
+ *
+ * Plain C types only: device pointers, sizes, a CUDA stream passed as void*
+ * (a cudaStream_t; NULL = legacy default stream).  Every entry point
+ * returns an int status (FTLE_OK = 0) and never throws; on error,
+ * ftle_last_error() returns a message for the calling thread.  The caller
+ * owns every buffer; no pointer is retained after a call returns.  Kernels
+ * are enqueued on `stream` and run asynchronously: synchronise the stream
+ * (or call ftle_stream_synchronize) before reading results on the host.
+ *
+ * Layouts (shared with pyFTLE):
+ *   positions  (K*N, dim) float64 row-major, role-blocked rows
+ *              [left(N); right(N); top(N); bottom(N) (; front(N); back(N))],
+ *              K = 2*dim neighbours per group (particles.py:153-237).
+ *   snapshot   (dim, nodes) float64, node (i,j) at j*nx+i in 2D and
+ *              (i,j,k) at (j*nx+i)*nz+k in 3D (meshgrid "xy" flattening,
+ *              the layout interpolate.py:359-401 un-flattens).
+ *   grid       origin = min coordinate per axis, spacing = (max-min)/(n-1)
+ *              computed on the host exactly as grid_interp.py:32-35 does.
+ */
+#ifndef PYFTLE_B200_H
+#define PYFTLE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  FTLE_OK = 0,
+  FTLE_ERR_INVALID = 1,     /* bad argument: null pointer, shape, unsupported combination */
+  FTLE_ERR_CUDA = 2,        /* a CUDA runtime call or launch failed */
+  FTLE_ERR_DEVICE = 3,      /* a kernel reported an error through its error word */
+  FTLE_ERR_UNSUPPORTED = 4  /* valid request this build does not implement */
+};
+
+enum { FTLE_EULER = 0, FTLE_AB2 = 1, FTLE_RK4 = 2 };    /* integrate.py:372-376 keys */
+enum { FTLE_HOLD = 0, FTLE_BLEND = 1 };                 /* time modes */
+enum { FTLE_F64 = 0, FTLE_F16 = 1, FTLE_BF16 = 2 };     /* snapshot storage */
+
+/* Regular grid of the "grid" interpolator (interpolate.py:342-425,
+ * grid_interp.py:30-38, 112-121). */
+typedef struct ftle_grid {
+  int32_t dim;         /* 2 or 3 */
+  int32_t n[3];        /* nodes per axis; n[2] ignored in 2D */
+  double origin[3];    /* grid_x[0], grid_y[0] (, grid_z[0]) */
+  double spacing[3];   /* (x[-1]-x[0])/(n-1) per axis */
+  int32_t periodic;    /* 0: velocity is 0 outside the grid (GridInterp.cpp:58,126);
+                          1: periodic wrap, node n == node 0 (no reference counterpart) */
+  int32_t reserved;
+} ftle_grid;
+
+/* One FTLE window: advect every particle, then Jacobian -> Cauchy-Green ->
+ * lambda_max -> FTLE per group.  Replaces FTLESolver.run
+ * (ftle_solver.py:68-120) with one launch. */
+typedef struct ftle_window {
+  ftle_grid grid;
+  const void *snapshots;   /* packed by ftle_pack_snapshots, num_snapshots records */
+  int32_t num_snapshots;
+  int32_t storage;         /* FTLE_F64 for ftle_window_run_f64; FTLE_F16/BF16 for _mixed */
+  int32_t time_mode;       /* FTLE_HOLD: step i holds snapshot first_snapshot+i (reference);
+                              FTLE_BLEND: linear blend of the snapshots around each stage time */
+  int32_t periodic_time;   /* BLEND/HOLD: snapshot index wraps modulo num_snapshots */
+  double snapshot_t0;      /* BLEND: time of snapshot 0 */
+  double snapshot_dt;      /* BLEND: spacing of the snapshots */
+  int32_t first_snapshot;  /* HOLD: snapshot used by step 0 */
+  int32_t integrator;      /* FTLE_EULER / FTLE_AB2 / FTLE_RK4 */
+  double t0;               /* BLEND: time of step 0 */
+  double h;                /* step; negative for backward time */
+  int32_t num_steps;
+  int32_t reserved;
+  double *positions;       /* (K*N, dim) in/out, role-blocked */
+  int64_t num_groups;      /* N */
+  double map_period;       /* T in FTLE = log(sqrt(lambda_max))/T; reference: (steps-1)*|dt| */
+  double *ftle;            /* N outputs, or NULL to skip the epilogue */
+} ftle_window;
+
+/* ---- library ----------------------------------------------------------- */
+int ftle_version(void);
+const char *ftle_last_error(void);
+int ftle_stream_synchronize(void *stream);
+
+/* ---- index-space gathers ------------------------------------------------
+ * Replace pyftle.ginterp.interp2d_vec_inplace / interp3d_vec_inplace
+ * (GridInterp.cpp:93-142 and :15-91, bound at :144-150): v is (nx, ny) or
+ * (X, Y, Z) C-contiguous, points (n, dim) in index space, out (n,).
+ * Bit-exact with the reference, including 0 outside the grid. */
+int ftle_interp2d_vec_inplace(const double *v, int32_t nx, int32_t ny, const double *points,
+                              int64_t n, double *out, void *stream);
+int ftle_interp3d_vec_inplace(const double *v, int32_t X, int32_t Y, int32_t Z,
+                              const double *points, int64_t n, double *out, void *stream);
+
+/* ---- grid interpolator --------------------------------------------------
+ * Replaces HighPerfInterpolator.interpolate (interpolate.py:475-543) together
+ * with Interp2D/3D.__call__ (grid_interp.py:40-85, 123-172): physical points
+ * (m, dim) -> velocities (m, dim) from one (dim, nodes) snapshot. */
+int ftle_grid_interpolate(const ftle_grid *grid, const double *snapshot, const double *points,
+                          int64_t m, double *out, void *stream);
+
+/* ---- one integrator step with the grid interpolator ---------------------
+ * Replaces EulerIntegrator / AdamsBashforth2Integrator /
+ * RungeKutta4Integrator.integrate (integrate.py:177-196, 223-257, 291-342)
+ * when the interpolator is the "grid" one: positions (m, dim) advance by h in
+ * place on the frozen snapshot.  AB2 only: `history` (m, dim) holds the
+ * previous velocity when history_valid != 0 (else the step is Euler) and
+ * receives this step's velocity. */
+int ftle_grid_step(const ftle_grid *grid, const double *snapshot, int32_t integrator, double h,
+                   double *positions, int64_t m, double *history, int32_t history_valid,
+                   void *stream);
+
+/* ---- integrator arithmetic for any interpolator --------------------------
+ * Bit-exact with the numpy / numba updates of integrate.py:
+ *   ftle_axpy:       out = x + a*k          (:327-339 stage points, :44 Euler)
+ *   ftle_ab2_update: x = x + h*(1.5*v - 0.5*v_prev)        (:78)
+ *   ftle_rk4_update: x = x + (h/6)*(k1 + 2k2 + 2k3 + k4)   (:109)
+ * n counts doubles. */
+int ftle_axpy(double *out, const double *x, double a, const double *k, int64_t n, void *stream);
+int ftle_ab2_update(double *x, double h, const double *v, const double *v_prev, int64_t n,
+                    void *stream);
+int ftle_rk4_update(double *x, double h, const double *k1, const double *k2, const double *k3,
+                    const double *k4, int64_t n, void *stream);
+
+/* ---- FTLE building blocks (cauchy_green.py, ftle.py) ---------------------
+ * initial_deltas: (dim, N, dim) = [right-left; top-bottom (; front-back)] at
+ * t0 (particles.py:85-100); only the diagonal entries are used
+ * (cauchy_green.py:70-74, 140-151).  J and C are (n, dim, dim). */
+int ftle_flow_map_jacobian(int32_t dim, const double *positions, const double *initial_deltas,
+                           int64_t num_groups, double *jacobian, void *stream);
+int ftle_cauchy_green(int32_t dim, const double *jacobian, int64_t n, double *cauchy_green,
+                      void *stream);
+int ftle_max_eigenvalue(int32_t dim, const double *cauchy_green, int64_t n, double *out,
+                        void *stream);
+int ftle_from_jacobian(int32_t dim, const double *jacobian, int64_t n, double map_period,
+                       double *out, void *stream);
+/* Jacobian -> C -> lambda_max -> FTLE in one pass (ftle_solver.py:122-161). */
+int ftle_from_positions(int32_t dim, const double *positions, const double *initial_deltas,
+                        int64_t num_groups, double map_period, double *out, void *stream);
+
+/* ---- fused windows -------------------------------------------------------
+ * Snapshots are first packed on the device: `src` is num_snapshots
+ * reference-layout snapshots back to back ((S, dim, nodes) float64);
+ * `dst` needs ftle_packed_snapshot_bytes(dim, nodes, S, storage) bytes and
+ * 256-byte alignment.  Record s holds snapshot s and its successor
+ * (s+1, or 0 when periodic_time, or s itself for the last one). */
+int64_t ftle_packed_snapshot_bytes(int32_t dim, int64_t nodes, int32_t num_snapshots,
+                                   int32_t storage);
+int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots,
+                        int32_t periodic_time, const double *src, int32_t storage, void *dst,
+                        void *stream);
+
+/* Plain FP64 window (storage FTLE_F64): reference arithmetic, one thread per
+ * particle, FTLE epilogue in the same kernel.  HOLD mode is bit-exact with
+ * pyFTLE's positions; FTLE within 1e-10 relative. */
+int ftle_window_run_f64(const ftle_window *w, void *stream);
+
+/* Mixed-precision window (storage FTLE_F16 or FTLE_BF16): FP32 advection of
+ * each group as an FP64 centroid plus FP32 neighbour offsets (split
+ * representation), FP64 Jacobian -> Cauchy-Green -> lambda_max.  Writes
+ * FP64 positions = centroid + offset. */
+int ftle_window_run_mixed(const ftle_window *w, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYFTLE_B200_H */

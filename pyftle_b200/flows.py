@@ -1,0 +1,203 @@
+"""Synthetic velocity fields and seed-particle layouts (host-side input builders).
+
+These build inputs in exactly the layouts pyFTLE consumes, so the same arrays
+drive the reference, the oracle and the CUDA engine:
+
+* a snapshot is ``(dim, nodes)`` float64 (``data_source.py`` / ``file_readers.py``);
+  2D node ``(i, j)`` is flattened as ``j*nx + i`` and 3D node ``(i, j, k)`` as
+  ``(j*nx + i)*nz + k`` -- numpy ``meshgrid(x, y[, z])`` ("xy" indexing)
+  followed by C-order ``ravel``, which is what ``interpolate.py:359-401``
+  un-flattens;
+* grid coordinates are the matching ``(dim, nodes)`` array;
+* neighbour particles are role-blocked ``(K*N, dim)`` rows
+  ``[left; right; top; bottom (; front; back)]`` (``particles.py:153-237``,
+  ``file_readers.py:175-180``).
+
+Flow formulas:
+
+* double gyre (``examples/01_Closed-form_velocity.ipynb`` of pyFTLE):
+  ``f = eps sin(wt) x^2 + (1 - 2 eps sin(wt)) x``,
+  ``u = -pi A sin(pi f) cos(pi y)``, ``v = pi A cos(pi f) sin(pi y) df/dx``;
+* time-periodic ABC: ``A(t) = A + 0.1 sin t``,
+  ``u = A(t) sin z + C cos y``, ``v = B sin x + A(t) cos z``,
+  ``w = C sin y + B cos x``;
+* 2D random-Fourier turbulence (divergence-free through a stream function,
+  energy spectrum ``E(k) ~ k^(-5/3)`` on ``4 <= |k| <= kmax``, seeded phases,
+  each mode with its own frequency).
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+# ----------------------------------------------------------------------------
+# grids and seeds
+# ----------------------------------------------------------------------------
+
+
+def grid_points_2d(nx: int, ny: int, xlim=(0.0, 2.0), ylim=(0.0, 1.0)) -> np.ndarray:
+    """(2, nx*ny) node coordinates, meshgrid 'xy' flattening (inclusive axes)."""
+    x = np.linspace(xlim[0], xlim[1], nx)
+    y = np.linspace(ylim[0], ylim[1], ny)
+    X, Y = np.meshgrid(x, y)
+    return np.stack((X.ravel(), Y.ravel()))
+
+
+def periodic_axis(n: int, length: float = 2.0 * math.pi) -> np.ndarray:
+    """n nodes of a periodic axis ``[0, length)`` (the endpoint is node 0 again)."""
+    return np.arange(n) * (length / n)
+
+
+def grid_points_3d(x: np.ndarray, y: np.ndarray, z: np.ndarray) -> np.ndarray:
+    """(3, nx*ny*nz) node coordinates, meshgrid 'xy' flattening."""
+    X, Y, Z = np.meshgrid(x, y, z)
+    return np.stack((X.ravel(), Y.ravel(), Z.ravel()))
+
+
+def seeds_2d(centroids: np.ndarray, delta: float) -> np.ndarray:
+    """Role-blocked (4N, 2) neighbours [L; R; T; B] around (N, 2) centroids."""
+    c = np.asarray(centroids, dtype=np.float64)
+    ex = np.array([delta, 0.0])
+    ey = np.array([0.0, delta])
+    return np.concatenate((c - ex, c + ex, c + ey, c - ey), axis=0)
+
+
+def seeds_3d(centroids: np.ndarray, delta: float) -> np.ndarray:
+    """Role-blocked (6N, 3) neighbours [L; R; T; B; F; Bk] around (N, 3) centroids."""
+    c = np.asarray(centroids, dtype=np.float64)
+    ex = np.array([delta, 0.0, 0.0])
+    ey = np.array([0.0, delta, 0.0])
+    ez = np.array([0.0, 0.0, delta])
+    return np.concatenate((c - ex, c + ex, c + ey, c - ey, c + ez, c - ez), axis=0)
+
+
+def centroid_grid_2d(ncx: int, ncy: int, xlim, ylim) -> np.ndarray:
+    """(N, 2) centroids on linspace axes, meshgrid 'xy' order."""
+    X, Y = np.meshgrid(np.linspace(*xlim, ncx), np.linspace(*ylim, ncy))
+    return np.column_stack((X.ravel(), Y.ravel()))
+
+
+def centroid_grid_3d(ncx: int, ncy: int, ncz: int, lo, hi) -> np.ndarray:
+    """(N, 3) centroids on linspace axes between lo and hi, meshgrid 'xy' order."""
+    X, Y, Z = np.meshgrid(np.linspace(lo[0], hi[0], ncx), np.linspace(lo[1], hi[1], ncy),
+                          np.linspace(lo[2], hi[2], ncz))
+    return np.column_stack((X.ravel(), Y.ravel(), Z.ravel()))
+
+
+# ----------------------------------------------------------------------------
+# double gyre
+# ----------------------------------------------------------------------------
+
+
+def double_gyre_velocity(t: float, pts: np.ndarray, A=0.1, eps=0.25, omega=2.0 * math.pi / 10.0):
+    """Velocity at (N, 2) points; same expression as pyFTLE's example notebook."""
+    x = pts[:, 0]
+    y = pts[:, 1]
+    s = math.sin(omega * t)
+    f = eps * s * x**2 + (1.0 - 2.0 * eps * s) * x
+    dfdx = 2 * eps * s * x + (1.0 - 2.0 * eps * s)
+    out = np.empty_like(pts, dtype=np.float64)
+    out[:, 0] = -np.pi * A * np.sin(np.pi * f) * np.cos(np.pi * y)
+    out[:, 1] = np.pi * A * np.cos(np.pi * f) * np.sin(np.pi * y) * dfdx
+    return out
+
+
+def double_gyre_snapshots(points: np.ndarray, times, **kw) -> np.ndarray:
+    """(S, 2, nodes) snapshots of the double gyre at ``times`` on grid ``points``."""
+    P = np.ascontiguousarray(points.T)
+    return np.stack([double_gyre_velocity(float(t), P, **kw).T.copy() for t in times])
+
+
+# ----------------------------------------------------------------------------
+# time-periodic ABC flow
+# ----------------------------------------------------------------------------
+
+ABC_A = math.sqrt(3.0)
+ABC_B = math.sqrt(2.0)
+ABC_C = 1.0
+
+
+def abc_velocity(t: float, pts: np.ndarray, A=ABC_A, B=ABC_B, C=ABC_C) -> np.ndarray:
+    At = A + 0.1 * math.sin(t)
+    x, y, z = pts[:, 0], pts[:, 1], pts[:, 2]
+    out = np.empty_like(pts, dtype=np.float64)
+    out[:, 0] = At * np.sin(z) + C * np.cos(y)
+    out[:, 1] = B * np.sin(x) + At * np.cos(z)
+    out[:, 2] = C * np.sin(y) + B * np.cos(x)
+    return out
+
+
+def abc_snapshots(x: np.ndarray, y: np.ndarray, z: np.ndarray, times, A=ABC_A, B=ABC_B,
+                  C=ABC_C, dtype=np.float64) -> np.ndarray:
+    """(S, 3, nx*ny*nz) ABC snapshots on the tensor grid x, y, z (separable build).
+
+    Node (i, j, k) sits at flat index (j*nx + i)*nz + k.
+    """
+    nx, ny, nz = len(x), len(y), len(z)
+    S = len(times)
+    out = np.empty((S, 3, ny, nx, nz), dtype=dtype)
+    sx, cx = np.sin(x), np.cos(x)
+    sy, cy = np.sin(y), np.cos(y)
+    sz, cz = np.sin(z), np.cos(z)
+    for s, t in enumerate(times):
+        At = A + 0.1 * math.sin(float(t))
+        out[s, 0] = (At * sz)[None, None, :] + (C * cy)[:, None, None]
+        out[s, 1] = (B * sx)[None, :, None] + (At * cz)[None, None, :]
+        out[s, 2] = (C * sy)[:, None, None] + (B * cx)[None, :, None]
+    return out.reshape(S, 3, nx * ny * nz)
+
+
+# ----------------------------------------------------------------------------
+# 2D random-Fourier turbulence
+# ----------------------------------------------------------------------------
+
+
+class FourierTurbulence2D:
+    """Divergence-free 2D random-mode field on the periodic box [0, L)^2.
+
+    psi(x, t) = sum_m a_m cos(k_m . x + phi_m + w_m t); u = dpsi/dy, v = -dpsi/dx.
+    Mode amplitudes follow E(k) ~ k^(-5/3) for integer wavenumbers
+    kmin <= |k| <= kmax; the field is normalised to unit rms speed.
+    """
+
+    def __init__(self, seed: int = 0, num_modes: int = 256, kmin: float = 4.0,
+                 kmax: float = 128.0, length: float = 2.0 * math.pi, omega_scale: float = 1.0):
+        rng = np.random.default_rng(seed)
+        self.length = length
+        kk = np.exp(rng.uniform(math.log(kmin), math.log(kmax), num_modes))
+        theta = rng.uniform(0.0, 2.0 * math.pi, num_modes)
+        k0 = 2.0 * math.pi / length
+        kx = np.round(kk * np.cos(theta))
+        ky = np.round(kk * np.sin(theta))
+        bad = (kx == 0) & (ky == 0)
+        kx[bad] = kmin
+        kmag = np.hypot(kx, ky)
+        # log-uniform sampling has density ~1/k, so E(k) ~ k^-5/3 needs
+        # amplitude^2 ~ k^-5/3 * k / k^2 (2D shell) -> psi amplitude ~ k^(-11/6) * k^(1/2)
+        amp = kmag ** (-5.0 / 6.0) / kmag
+        self.kx = kx * k0
+        self.ky = ky * k0
+        self.phase = rng.uniform(0.0, 2.0 * math.pi, num_modes)
+        self.omega = omega_scale * rng.standard_normal(num_modes)
+        # normalise rms speed to 1
+        speed2 = 0.5 * np.sum((amp * self.kx) ** 2 + (amp * self.ky) ** 2)
+        self.amp = amp / math.sqrt(speed2)
+
+    def snapshot(self, n: int, t: float) -> np.ndarray:
+        """(2, n*n) velocity on the n x n periodic grid (j*n + i flattening)."""
+        x = periodic_axis(n, self.length)
+        u = np.zeros((n, n))
+        v = np.zeros((n, n))
+        for m in range(len(self.amp)):
+            ph = self.phase[m] + self.omega[m] * t
+            cx = np.exp(1j * (self.kx[m] * x))  # along i (x)
+            cy = np.exp(1j * (self.ky[m] * x + ph))  # along j (y)
+            s = -np.imag(np.outer(cy, cx))  # sin(kx x + ky y + ph) at [j, i]
+            u += self.amp[m] * (-self.ky[m]) * s
+            v += self.amp[m] * (self.kx[m]) * s
+        return np.stack((u.ravel(), v.ravel()))
+
+    def snapshots(self, n: int, times) -> np.ndarray:
+        return np.stack([self.snapshot(n, float(t)) for t in times])
