@@ -49,7 +49,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--precision", choices=["fp16", "bf16", "fp64"], default="fp16")
+    p.add_argument("--precision", choices=["fx15", "fp16", "bf16", "fp64"], default="fx15")
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--snapshots", type=int, default=64)
     p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
@@ -382,7 +382,7 @@ def run_ours(args):
         peak_src = "measured"
     except Exception:
         peak, peak_src = 6650.0, "fallback"
-    elem = 2 if args.precision in ("fp16", "bf16") else 8
+    elem = 2 if args.precision in ("fx15", "fp16", "bf16") else 8
     bytes_per_ps = 4 * 8 * 3 * 2 * elem  # stages x corners x comps x snapshots x elem
     achieved = bytes_per_ps * particle_steps / (kernel_ms / 1e3) / 1e9
     traffic = None

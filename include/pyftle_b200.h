@@ -39,7 +39,10 @@ enum {
 
 enum { FTLE_EULER = 0, FTLE_AB2 = 1, FTLE_RK4 = 2 };    /* integrate.py:372-376 keys */
 enum { FTLE_HOLD = 0, FTLE_BLEND = 1 };                 /* time modes */
-enum { FTLE_F64 = 0, FTLE_F16 = 1, FTLE_BF16 = 2 };     /* snapshot storage */
+/* Snapshot storage.  FTLE_FX15: 15-bit fixed point per component over the
+ * series' value range (uniform absolute error range/65534; decoded by one
+ * byte permute into an FP32 in [0.5, 1)). */
+enum { FTLE_F64 = 0, FTLE_F16 = 1, FTLE_BF16 = 2, FTLE_FX15 = 3 };
 
 /* Regular grid of the "grid" interpolator (interpolate.py:342-425,
  * grid_interp.py:30-38, 112-121). */
@@ -60,7 +63,7 @@ typedef struct ftle_window {
   ftle_grid grid;
   const void *snapshots;   /* packed by ftle_pack_snapshots, num_snapshots records */
   int32_t num_snapshots;
-  int32_t storage;         /* FTLE_F64 for ftle_window_run_f64; FTLE_F16/BF16 for _mixed */
+  int32_t storage;         /* FTLE_F64 for ftle_window_run_f64; FTLE_F16/BF16/FX15 for _mixed */
   int32_t time_mode;       /* FTLE_HOLD: step i holds snapshot first_snapshot+i (reference);
                               FTLE_BLEND: linear blend of the snapshots around each stage time */
   int32_t periodic_time;   /* BLEND/HOLD: snapshot index wraps modulo num_snapshots */
@@ -143,8 +146,10 @@ int ftle_from_positions(int32_t dim, const double *positions, const double *init
  * Snapshots are first packed on the device: `src` is num_snapshots
  * reference-layout snapshots back to back ((S, dim, nodes) float64);
  * `dst` needs ftle_packed_snapshot_bytes(dim, nodes, S, storage) bytes and
- * 256-byte alignment.  Record s holds snapshot s and its successor
- * (s+1, or 0 when periodic_time, or s itself for the last one). */
+ * 16-byte alignment.  Record s holds snapshot s and its successor
+ * (s+1, or 0 when periodic_time, or s itself for the last one).  The 16-bit
+ * storages start with a 256-byte header (per-component decode scale and
+ * offset) followed by the records. */
 int64_t ftle_packed_snapshot_bytes(int32_t dim, int64_t nodes, int32_t num_snapshots,
                                    int32_t storage);
 int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots,
@@ -156,7 +161,7 @@ int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots,
  * pyFTLE's positions; FTLE within 1e-10 relative. */
 int ftle_window_run_f64(const ftle_window *w, void *stream);
 
-/* Mixed-precision window (storage FTLE_F16 or FTLE_BF16): FP32 advection of
+/* Mixed-precision window (storage FTLE_F16, FTLE_BF16 or FTLE_FX15): FP32 advection of
  * each group as an FP64 centroid plus FP32 neighbour offsets (split
  * representation), FP64 Jacobian -> Cauchy-Green -> lambda_max.  Writes
  * FP64 positions = centroid + offset. */

@@ -61,8 +61,9 @@ int window_to_kernel(const ftle_window *w, WinK *k) {
   if (!w) return fail_invalid("window descriptor is NULL");
   int rc = grid_from_abi(&w->grid, &k->g);
   if (rc) return rc;
-  if (!w->snapshots || !w->positions) return fail_invalid("snapshots and positions are required");
   if (w->num_groups < 0) return fail_invalid("num_groups must be >= 0");
+  if (!w->snapshots) return fail_invalid("snapshots are required");
+  if (!w->positions && w->num_groups > 0) return fail_invalid("positions are required");
   if (w->num_steps < 0) return fail_invalid("num_steps must be >= 0");
   if (w->integrator < FTLE_EULER || w->integrator > FTLE_RK4)
     return fail_invalid("unknown integrator %d", w->integrator);
@@ -121,14 +122,13 @@ int ftle_stream_synchronize(void *stream) {
 int64_t ftle_packed_snapshot_bytes(int32_t dim, int64_t nodes, int32_t num_snapshots,
                                    int32_t storage) {
   if ((dim != 2 && dim != 3) || nodes < 0 || num_snapshots < 0) return -1;
-  int64_t rec;
-  if (storage == FTLE_F64)
-    rec = 2 * dim * 8;  // [snapshot s | successor] doubles
-  else if (storage == FTLE_F16 || storage == FTLE_BF16)
-    rec = dim == 2 ? 8 : 16;  // 4 or 8 16-bit values (3D pads each half to 4)
-  else
-    return -1;
-  return rec * nodes * num_snapshots;
+  if (storage == FTLE_F64) return (int64_t)(2 * dim * 8) * nodes * num_snapshots;
+  if (storage == FTLE_F16 || storage == FTLE_BF16 || storage == FTLE_FX15) {
+    // 256-byte decode header, then 4 or 8 16-bit values per record (3D pads each half to 4)
+    const int64_t rec = dim == 2 ? 8 : 16;
+    return 256 + rec * nodes * num_snapshots;
+  }
+  return -1;
 }
 
 int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots, int32_t periodic_time,
@@ -141,7 +141,7 @@ int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots, int32
   if (storage == FTLE_F64)
     return pack_snapshots_f64(dim, nodes, num_snapshots, periodic_time, src,
                               static_cast<double *>(dst), stream);
-  if (storage == FTLE_F16 || storage == FTLE_BF16)
+  if (storage == FTLE_F16 || storage == FTLE_BF16 || storage == FTLE_FX15)
     return pack_snapshots_16(dim, nodes, num_snapshots, periodic_time, src, storage, dst, stream);
   return fail_invalid("unknown storage %d", storage);
 }

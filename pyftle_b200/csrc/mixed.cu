@@ -1,18 +1,26 @@
 // mixed.cu -- mixed-precision FTLE window (sm_100a).
 //
-// Snapshots are stored as FP16 or BF16 "pair records": record (s, node) holds
-// the velocity of snapshot s and of its successor, so one 8-byte (2D) or
-// 16-byte (3D) load per cell corner serves a time-blended gather.
+// Storage: 16-bit "pair records": record (s, node) holds the velocity of
+// snapshot s and of its successor, so one 8-byte (2D) or 16-byte (3D) load per
+// cell corner serves a time-blended gather.  Three encodings:
+//   FTLE_F16 / FTLE_BF16  IEEE half / bfloat16 velocities;
+//   FTLE_FX15             15-bit fixed point per component over the series'
+//                         value range: one byte permute turns a value into the
+//                         FP32 0.5 + q/65536, and u = scale*f + offset.
+// A 256-byte header in front of the records holds scale/offset per component.
 //
-// Each thread advects one neighbour group in the split representation:
-//   centroid c            FP64 (its cell index and in-cell fraction are exact)
-//   offsets  d_k = x_k-c  FP32, advected with velocity differences u(x_k)-u(c)
-// so the finite differences x_R - x_L never cancel in FP32.  Velocities are
-// FP32 (blend in time at the corners, then bi/trilinear).  The 8 (3D) or 4
-// (2D) corner values of the centroid's cell stay in registers and serve every
-// neighbour that sits in the same cell, which is nearly all of them while the
-// group is smaller than a cell.  The Jacobian -> Cauchy-Green -> lambda_max
-// epilogue runs in FP64 (ftle.py:9-233 restated).
+// Work unit: one thread advects one neighbour group in the split
+// representation
+//   centroid c           FP64 -> its cell index and in-cell fraction are exact
+//   offsets  d_k = x_k-c FP32, advected with velocity differences u(c+d_k)-u(c)
+// so x_R - x_L never cancels in FP32.  Per RK4 stage the thread gathers the
+// centroid's cell once, turns its (time-blended) corners into the cell's
+// multilinear polynomial, and evaluates every neighbour inside that cell as an
+// exact polynomial *difference* p(f+delta) - p(f) (no FP32 cancellation).
+// Neighbours that left the cell go through one shared gather loop.  The stage
+// loop is a runtime loop so the kernel body stays small (instruction-cache
+// resident).  Jacobian -> Cauchy-Green -> lambda_max runs in FP64
+// (ftle.py:9-233 restated).
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <math.h>
@@ -21,276 +29,343 @@
 
 namespace ftle {
 
+constexpr int kHeaderBytes = 256;
+constexpr int kFxMax = 32767;  // 15-bit fixed point
+
+struct Header16 {
+  float scale[4];
+  float offset[4];
+  float vmin[4];
+  float vmax[4];
+};
+
 // ---------------------------------------------------------------------------
-// 16-bit storage traits
+// decoding two 16-bit values held in one 32-bit word
 // ---------------------------------------------------------------------------
 template <int STORAGE>
-struct Half2;  // unpack two 16-bit values packed in a 32-bit word
+struct Dec;
 
 template <>
-struct Half2<FTLE_F16> {
-  static __device__ __forceinline__ float2 unpack(unsigned w) {
-    __half2 h;
-    memcpy(&h, &w, 4);
-    return __half22float2(h);
+struct Dec<FTLE_F16> {
+  static __device__ __forceinline__ float lo(unsigned w) {
+    return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
   }
-  static __device__ __forceinline__ unsigned short from_double(double x) {
-    __half h = __double2half(x);
-    unsigned short b;
-    memcpy(&b, &h, 2);
-    return b;
+  static __device__ __forceinline__ float hi(unsigned w) {
+    return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+  }
+  static __device__ __forceinline__ unsigned short enc(double x, const Header16 &) {
+    return __half_as_ushort(__double2half(x));
   }
 };
 
 template <>
-struct Half2<FTLE_BF16> {
-  static __device__ __forceinline__ float2 unpack(unsigned w) {
-    return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+struct Dec<FTLE_BF16> {
+  static __device__ __forceinline__ float lo(unsigned w) { return __uint_as_float(w << 16); }
+  static __device__ __forceinline__ float hi(unsigned w) {
+    return __uint_as_float(w & 0xffff0000u);
   }
-  static __device__ __forceinline__ unsigned short from_double(double x) {
-    __nv_bfloat16 h = __double2bfloat16(x);
-    unsigned short b;
-    memcpy(&b, &h, 2);
-    return b;
+  static __device__ __forceinline__ unsigned short enc(double x, const Header16 &) {
+    return __bfloat16_as_ushort(__double2bfloat16(x));
   }
 };
 
+// bits 0x3F000000 | q << 8 is the float 0.5 + q/65536 for q < 2^15
+template <>
+struct Dec<FTLE_FX15> {
+  static __device__ __forceinline__ float lo(unsigned w) {
+    return __uint_as_float(__byte_perm(w, 0x3F000000u, 0x7104));
+  }
+  static __device__ __forceinline__ float hi(unsigned w) {
+    return __uint_as_float(__byte_perm(w, 0x3F000000u, 0x7324));
+  }
+  static __device__ __forceinline__ unsigned short enc(double x, const Header16 &h) = delete;
+};
+
 // ---------------------------------------------------------------------------
-// packing: (S, dim, nodes) float64 -> pair records
+// packing (S, dim, nodes) float64 -> header + pair records
 // ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void atomic_min_f(float *a, float v) {
+  if (v >= 0.0f)
+    atomicMin(reinterpret_cast<int *>(a), __float_as_int(v));
+  else
+    atomicMax(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+__device__ __forceinline__ void atomic_max_f(float *a, float v) {
+  if (v >= 0.0f)
+    atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
+  else
+    atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
+}
+
+__global__ void header_init_kernel(Header16 *h) {
+  const int c = threadIdx.x;
+  if (c < 4) {
+    h->scale[c] = 1.0f;
+    h->offset[c] = 0.0f;
+    h->vmin[c] = __int_as_float(0x7f800000);   // +inf
+    h->vmax[c] = __int_as_float(0xff800000);   // -inf
+  }
+}
+
+// per-component min / max over every snapshot and node
+template <int DIM>
+__global__ void minmax_kernel(const double *__restrict__ src, long long nodes, int S, Header16 *h) {
+  float mn[DIM], mx[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    mn[c] = __int_as_float(0x7f800000);
+    mx[c] = __int_as_float(0xff800000);
+  }
+  const long long total = nodes * S;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = i / nodes, p = i - s * nodes;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const double v = src[(s * DIM + c) * nodes + p];
+      mn[c] = fminf(mn[c], __double2float_rd(v));
+      mx[c] = fmaxf(mx[c], __double2float_ru(v));
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[c] = fminf(mn[c], __shfl_xor_sync(0xffffffffu, mn[c], o));
+      mx[c] = fmaxf(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomic_min_f(&h->vmin[c], mn[c]);
+      atomic_max_f(&h->vmax[c], mx[c]);
+    }
+  }
+}
+
+// u = scale * (0.5 + q/65536) + offset  with  q = (v - vmin) / step,  step = range / 32767
+__global__ void fx_finalize_kernel(Header16 *h, int dim) {
+  const int c = threadIdx.x;
+  if (c < dim) {
+    const double range = (double)h->vmax[c] - (double)h->vmin[c];
+    const double step = range > 0.0 ? range / kFxMax : 0.0;
+    const double S = 65536.0 * step;
+    h->scale[c] = (float)S;
+    h->offset[c] = (float)((double)h->vmin[c] - 0.5 * S);
+  }
+}
+
+template <int STORAGE>
+__device__ __forceinline__ unsigned short encode(double v, const Header16 &h, int c) {
+  if constexpr (STORAGE == FTLE_FX15) {
+    const double range = (double)h.vmax[c] - (double)h.vmin[c];
+    double q = range > 0.0 ? rint((v - (double)h.vmin[c]) * (kFxMax / range)) : 0.0;
+    q = q < 0.0 ? 0.0 : (q > kFxMax ? kFxMax : q);
+    return (unsigned short)q;
+  } else {
+    return Dec<STORAGE>::enc(v, h);
+  }
+}
+
 template <int DIM, int STORAGE>
 __global__ void pack16_kernel(const double *__restrict__ src, long long nodes, int S,
-                              int periodic_time, unsigned short *dst) {
-  constexpr int W = DIM == 2 ? 4 : 8;  // 16-bit values per record
+                              int periodic_time, const Header16 *__restrict__ hdr,
+                              unsigned char *recs) {
+  const Header16 h = *hdr;
   const long long total = nodes * S;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     const int s = (int)(i / nodes);
     const long long p = i - (long long)s * nodes;
     const int s1 = (s + 1 < S) ? s + 1 : (periodic_time ? 0 : s);
-    unsigned short r[W];
-    const int half = W / 2;
+    unsigned short a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
 #pragma unroll
-    for (int c = 0; c < half; ++c) {
-      r[c] = c < DIM ? Half2<STORAGE>::from_double(src[((long long)s * DIM + c) * nodes + p]) : 0;
-      r[half + c] =
-          c < DIM ? Half2<STORAGE>::from_double(src[((long long)s1 * DIM + c) * nodes + p]) : 0;
+    for (int c = 0; c < DIM; ++c) {
+      a[c] = encode<STORAGE>(src[((long long)s * DIM + c) * nodes + p], h, c);
+      b[c] = encode<STORAGE>(src[((long long)s1 * DIM + c) * nodes + p], h, c);
     }
     if constexpr (DIM == 2) {
       uint2 v;
-      v.x = (unsigned)r[0] | ((unsigned)r[1] << 16);
-      v.y = (unsigned)r[2] | ((unsigned)r[3] << 16);
-      reinterpret_cast<uint2 *>(dst)[i] = v;
+      v.x = (unsigned)a[0] | ((unsigned)a[1] << 16);
+      v.y = (unsigned)b[0] | ((unsigned)b[1] << 16);
+      reinterpret_cast<uint2 *>(recs)[i] = v;
     } else {
       uint4 v;
-      v.x = (unsigned)r[0] | ((unsigned)r[1] << 16);
-      v.y = (unsigned)r[2] | ((unsigned)r[3] << 16);
-      v.z = (unsigned)r[4] | ((unsigned)r[5] << 16);
-      v.w = (unsigned)r[6] | ((unsigned)r[7] << 16);
-      reinterpret_cast<uint4 *>(dst)[i] = v;
+      v.x = (unsigned)a[0] | ((unsigned)a[1] << 16);
+      v.y = (unsigned)a[2];
+      v.z = (unsigned)b[0] | ((unsigned)b[1] << 16);
+      v.w = (unsigned)b[2];
+      reinterpret_cast<uint4 *>(recs)[i] = v;
     }
   }
+}
+
+template <int DIM, int STORAGE>
+static int pack16(int64_t nodes, int32_t S, int32_t periodic_time, const double *src, void *dst,
+                  cudaStream_t st) {
+  Header16 *h = static_cast<Header16 *>(dst);
+  unsigned char *recs = static_cast<unsigned char *>(dst) + kHeaderBytes;
+  header_init_kernel<<<1, 32, 0, st>>>(h);
+  if constexpr (STORAGE == FTLE_FX15) {
+    minmax_kernel<DIM><<<grid_blocks(nodes * S, 256), 256, 0, st>>>(src, nodes, S, h);
+    fx_finalize_kernel<<<1, 32, 0, st>>>(h, DIM);
+  }
+  pack16_kernel<DIM, STORAGE><<<grid_blocks(nodes * S, 256), 256, 0, st>>>(src, nodes, S,
+                                                                           periodic_time, h, recs);
+  return check_launch("pack16_kernel");
 }
 
 int pack_snapshots_16(int32_t dim, int64_t nodes, int32_t num_snapshots, int32_t periodic_time,
                       const double *src, int32_t storage, void *dst, void *stream) {
-  const int64_t total = nodes * num_snapshots;
-  const unsigned b = grid_blocks(total, 256);
   cudaStream_t st = as_stream(stream);
-  unsigned short *d = static_cast<unsigned short *>(dst);
+#define P16(D, S) return pack16<D, S>(nodes, num_snapshots, periodic_time, src, dst, st)
   if (dim == 2) {
-    if (storage == FTLE_F16)
-      pack16_kernel<2, FTLE_F16><<<b, 256, 0, st>>>(src, nodes, num_snapshots, periodic_time, d);
-    else
-      pack16_kernel<2, FTLE_BF16><<<b, 256, 0, st>>>(src, nodes, num_snapshots, periodic_time, d);
+    if (storage == FTLE_F16) P16(2, FTLE_F16);
+    if (storage == FTLE_BF16) P16(2, FTLE_BF16);
+    P16(2, FTLE_FX15);
   } else {
-    if (storage == FTLE_F16)
-      pack16_kernel<3, FTLE_F16><<<b, 256, 0, st>>>(src, nodes, num_snapshots, periodic_time, d);
-    else
-      pack16_kernel<3, FTLE_BF16><<<b, 256, 0, st>>>(src, nodes, num_snapshots, periodic_time, d);
+    if (storage == FTLE_F16) P16(3, FTLE_F16);
+    if (storage == FTLE_BF16) P16(3, FTLE_BF16);
+    P16(3, FTLE_FX15);
   }
-  return check_launch("pack16_kernel");
+#undef P16
 }
 
 // ---------------------------------------------------------------------------
-// gathers
+// window kernel
 // ---------------------------------------------------------------------------
+
+constexpr int kBlock = 128;
 
 struct MixK {
   WinK w;
-  double inv_sp[3];   // 1/spacing (FP64, centroid cell)
-  float inv_spf[3];   // 1/spacing (FP32, neighbour offsets)
-  double inv_dt;      // 1/snapshot_dt
+  double inv_sp[3];   // 1/spacing
+  double org_sp[3];   // origin/spacing: p = x*inv_sp - org_sp
+  float inv_spf[3];
+  double inv_dt;
 };
 
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
 
-// Blended corner velocities of cell (i0) -> v[corner][comp], corner order
-// x0y0(z0) x1y0 x0y1 x1y1 (then the same at z1).
-template <int DIM, bool BLEND, int STORAGE>
-__device__ __forceinline__ void gather_cell(const GridK &g, const void *__restrict__ base,
-                                            float alpha, const int *i0, float (*v)[DIM]) {
+// Time-blended corner values v[c][q] of the cell whose lower corner is `cell`
+// (q = x + 2y (+ 4z)); false if the cell is outside a non-periodic grid.
+template <int DIM, int STORAGE, bool BLEND>
+__device__ __forceinline__ bool cell_values(const GridK &g, const unsigned char *__restrict__ recs,
+                                            float alpha, const int *cell, float (*v)[1 << DIM]) {
   int lo[DIM], hi[DIM];
 #pragma unroll
   for (int a = 0; a < DIM; ++a) {
-    lo[a] = i0[a];
-    hi[a] = i0[a] + 1;
     if (g.periodic) {
-      lo[a] = wrap_index(lo[a], g.n[a]);
+      lo[a] = wrap_index(cell[a], g.n[a]);
       hi[a] = lo[a] + 1 == g.n[a] ? 0 : lo[a] + 1;
+    } else {
+      if (cell[a] < 0 || cell[a] > g.n[a] - 2) return false;
+      lo[a] = cell[a];
+      hi[a] = cell[a] + 1;
     }
   }
-  if constexpr (DIM == 2) {
-    const uint2 *rec = static_cast<const uint2 *>(base);
-    long long nd[4] = {node2(g, lo[0], lo[1]), node2(g, hi[0], lo[1]), node2(g, lo[0], hi[1]),
-                       node2(g, hi[0], hi[1])};
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const uint2 r = __ldg(rec + nd[q]);
-      const float2 a = Half2<STORAGE>::unpack(r.x);
-      if constexpr (BLEND) {
-        const float2 b = Half2<STORAGE>::unpack(r.y);
-        v[q][0] = lerpf(a.x, b.x, alpha);
-        v[q][1] = lerpf(a.y, b.y, alpha);
-      } else {
-        v[q][0] = a.x;
-        v[q][1] = a.y;
-      }
-    }
-  } else {
-    const uint4 *rec = static_cast<const uint4 *>(base);
-    long long nd[8] = {node3(g, lo[0], lo[1], lo[2]), node3(g, hi[0], lo[1], lo[2]),
-                       node3(g, lo[0], hi[1], lo[2]), node3(g, hi[0], hi[1], lo[2]),
-                       node3(g, lo[0], lo[1], hi[2]), node3(g, hi[0], lo[1], hi[2]),
-                       node3(g, lo[0], hi[1], hi[2]), node3(g, hi[0], hi[1], hi[2])};
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const uint4 r = __ldg(rec + nd[q]);
-      const float2 a = Half2<STORAGE>::unpack(r.x);
-      const float2 aw = Half2<STORAGE>::unpack(r.y);
-      if constexpr (BLEND) {
-        const float2 b = Half2<STORAGE>::unpack(r.z);
-        const float2 bw = Half2<STORAGE>::unpack(r.w);
-        v[q][0] = lerpf(a.x, b.x, alpha);
-        v[q][1] = lerpf(a.y, b.y, alpha);
-        v[q][2] = lerpf(aw.x, bw.x, alpha);
-      } else {
-        v[q][0] = a.x;
-        v[q][1] = a.y;
-        v[q][2] = aw.x;
-      }
-    }
-  }
-}
-
-template <int DIM>
-__device__ __forceinline__ void interp_cell(const float (*v)[DIM], const float *f, float *u) {
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    const float x0 = lerpf(v[0][c], v[1][c], f[0]);
-    const float x1 = lerpf(v[2][c], v[3][c], f[0]);
-    const float y0 = lerpf(x0, x1, f[1]);
+  for (int q = 0; q < (1 << DIM); ++q) {
+    const int i = (q & 1) ? hi[0] : lo[0];
+    const int j = (q & 2) ? hi[1] : lo[1];
     if constexpr (DIM == 2) {
-      u[c] = y0;
+      const uint2 r = __ldg(reinterpret_cast<const uint2 *>(recs) + node2(g, i, j));
+      const float u0 = Dec<STORAGE>::lo(r.x), v0 = Dec<STORAGE>::hi(r.x);
+      if constexpr (BLEND) {
+        v[0][q] = lerpf(u0, Dec<STORAGE>::lo(r.y), alpha);
+        v[1][q] = lerpf(v0, Dec<STORAGE>::hi(r.y), alpha);
+      } else {
+        v[0][q] = u0;
+        v[1][q] = v0;
+      }
     } else {
-      const float x2 = lerpf(v[4][c], v[5][c], f[0]);
-      const float x3 = lerpf(v[6][c], v[7][c], f[0]);
-      const float y1 = lerpf(x2, x3, f[1]);
-      u[c] = lerpf(y0, y1, f[2]);
+      const int k = (q & 4) ? hi[2] : lo[2];
+      const uint4 r = __ldg(reinterpret_cast<const uint4 *>(recs) + node3(g, i, j, k));
+      const float u0 = Dec<STORAGE>::lo(r.x), v0 = Dec<STORAGE>::hi(r.x);
+      const float w0 = Dec<STORAGE>::lo(r.y);
+      if constexpr (BLEND) {
+        v[0][q] = lerpf(u0, Dec<STORAGE>::lo(r.z), alpha);
+        v[1][q] = lerpf(v0, Dec<STORAGE>::hi(r.z), alpha);
+        v[2][q] = lerpf(w0, Dec<STORAGE>::lo(r.w), alpha);
+      } else {
+        v[0][q] = u0;
+        v[1][q] = v0;
+        v[2][q] = w0;
+      }
     }
+  }
+  return true;
+}
+
+// multilinear interpolation by lerps (x, then y, then z)
+template <int DIM>
+__device__ __forceinline__ float interp_lerp(const float *v, const float *f) {
+  const float x0 = lerpf(v[0], v[1], f[0]);
+  const float x1 = lerpf(v[2], v[3], f[0]);
+  const float y0 = lerpf(x0, x1, f[1]);
+  if constexpr (DIM == 2) {
+    return y0;
+  } else {
+    const float x2 = lerpf(v[4], v[5], f[0]);
+    const float x3 = lerpf(v[6], v[7], f[0]);
+    return lerpf(y0, lerpf(x2, x3, f[1]), f[2]);
+  }
+}
+
+// p(x) = a0 + a1 x + a2 y (+ a3 z) + a4 xy + a5 xz + a6 yz + a7 xyz  (2D: a0 a1 a2 a3=xy)
+template <int DIM>
+__device__ __forceinline__ void poly_setup(const float *v, float *A) {
+  if constexpr (DIM == 2) {
+    A[0] = v[0];
+    A[1] = v[1] - v[0];
+    A[2] = v[2] - v[0];
+    A[3] = (v[3] - v[2]) - (v[1] - v[0]);
+  } else {
+    A[0] = v[0];
+    A[1] = v[1] - v[0];
+    A[2] = v[2] - v[0];
+    A[3] = v[4] - v[0];
+    A[4] = (v[3] - v[1]) - A[2];
+    A[5] = (v[5] - v[1]) - A[3];
+    A[6] = (v[6] - v[2]) - A[3];
+    A[7] = ((v[7] - v[6]) - (v[5] - v[4])) - ((v[3] - v[2]) - (v[1] - v[0]));
   }
 }
 
 template <int DIM>
-__device__ __forceinline__ bool cell_inside(const GridK &g, const int *i0) {
-  if (g.periodic) return true;
-  bool in = true;
-#pragma unroll
-  for (int a = 0; a < DIM; ++a) in = in && i0[a] >= 0 && i0[a] <= g.n[a] - 2;
-  return in;
+__device__ __forceinline__ float poly_eval(const float *A, const float *f) {
+  if constexpr (DIM == 2) {
+    return fmaf(f[0], fmaf(f[1], A[3], A[1]), fmaf(f[1], A[2], A[0]));
+  } else {
+    const float x = f[0], y = f[1], z = f[2];
+    const float t1 = fmaf(z, A[7], A[4]);
+    const float t3 = fmaf(z, A[5], fmaf(y, t1, A[1]));
+    const float t4 = fmaf(z, A[6], A[2]);
+    return fmaf(z, A[3], fmaf(y, t4, fmaf(x, t3, A[0])));
+  }
 }
 
-// Velocity of the centroid (uc) and velocity differences du[k] = u(c + d_k) - u(c).
-template <int DIM, bool BLEND, int STORAGE>
-__device__ __forceinline__ void eval_group(const MixK &m, const void *base, float alpha,
-                                           const double *cs, const float (*ds)[DIM], float *uc,
-                                           float (*du)[DIM]) {
-  constexpr int K = 2 * DIM;
-  const GridK &g = m.w.g;
-  int ci[DIM];
-  float fc[DIM];
-  bool finite = true;
-#pragma unroll
-  for (int a = 0; a < DIM; ++a) {
-    const double p = (cs[a] - g.origin[a]) * m.inv_sp[a];
-    const double fl = floor(p);
-    finite = finite && fabs(fl) < 1.0e9;
-    ci[a] = finite ? (int)fl : 0;
-    fc[a] = finite ? (float)(p - fl) : 0.0f;
-  }
-  if (!finite) {  // far outside or NaN: the whole group stands still
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) uc[a] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) du[k][a] = 0.0f;
-    return;
-  }
-  float v[1 << DIM][DIM];
-  const bool cin = cell_inside<DIM>(g, ci);
-  if (cin) {
-    gather_cell<DIM, BLEND, STORAGE>(g, base, alpha, ci, v);
-    interp_cell<DIM>(v, fc, uc);
+// p(f + d) - p(f), written so that no large terms cancel
+template <int DIM>
+__device__ __forceinline__ float poly_diff(const float *A, const float *f, const float *d,
+                                           const float *F) {  // F = f + d
+  if constexpr (DIM == 2) {
+    // a1 dx + a2 dy + a3 (dx Y' + x dy)
+    return fmaf(d[0], fmaf(A[3], F[1], A[1]), d[1] * fmaf(A[3], f[0], A[2]));
   } else {
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) uc[a] = 0.0f;
-  }
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    float q[DIM];
-    int o[DIM];
-    bool same = true;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-      const float qa = fmaf(ds[k][a], m.inv_spf[a], fc[a]);
-      const float fo = floorf(qa);
-      o[a] = (int)fo;
-      q[a] = qa - fo;
-      same = same && o[a] == 0;
-    }
-    float uk[DIM];
-    if (same) {
-      if (cin) {
-        interp_cell<DIM>(v, q, uk);
-      } else {
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) uk[a] = 0.0f;
-      }
-    } else {
-      int ck[DIM];
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) ck[a] = ci[a] + o[a];
-      if (cell_inside<DIM>(g, ck)) {
-        float vk[1 << DIM][DIM];
-        gather_cell<DIM, BLEND, STORAGE>(g, base, alpha, ck, vk);
-        interp_cell<DIM>(vk, q, uk);
-      } else {
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) uk[a] = 0.0f;
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) du[k][a] = uk[a] - uc[a];
+    const float x = f[0], y = f[1];
+    const float Y = F[1], Z = F[2];
+    const float t = fmaf(A[7], Z, A[4]);
+    const float gx = fmaf(Y, t, fmaf(A[5], Z, A[1]));
+    const float gy = fmaf(x, t, fmaf(A[6], Z, A[2]));
+    const float gz = fmaf(x, fmaf(A[7], y, A[5]), fmaf(A[6], y, A[3]));
+    return fmaf(d[0], gx, fmaf(d[1], gy, d[2] * gz));
   }
 }
 
 template <int DIM, int MODE>
-__device__ __forceinline__ const void *record_set(const MixK &m, int step, double t,
-                                                  float &alpha) {
+__device__ __forceinline__ const unsigned char *record_set(const MixK &m, int step, double t,
+                                                           float &alpha) {
   const long long rec_bytes = DIM == 2 ? 8 : 16;
-  const char *base = static_cast<const char *>(m.w.snaps);
-  const long long set_bytes = m.w.g.nodes * rec_bytes;
+  const unsigned char *base = static_cast<const unsigned char *>(m.w.snaps) + kHeaderBytes;
   int s;
   if constexpr (MODE == FTLE_HOLD) {
     s = m.w.first_snapshot + step;
@@ -315,12 +390,12 @@ __device__ __forceinline__ const void *record_set(const MixK &m, int step, doubl
       alpha = (float)(tau - (double)s);
     }
   }
-  return base + (long long)s * set_bytes;
+  return base + (long long)s * m.w.g.nodes * rec_bytes;
 }
 
-// ---------------------------------------------------------------------------
-// FP64 epilogue (same formulas as the plain path)
-// ---------------------------------------------------------------------------
+__device__ __forceinline__ int plus_r(int j) { return j == 0 ? 1 : 2 * j; }
+__device__ __forceinline__ int minus_r(int j) { return j == 0 ? 0 : 2 * j + 1; }
+
 __device__ __forceinline__ double lmax2(double F00, double F01, double F10, double F11) {
   const double A = F00 * F00 + F10 * F10;
   const double B = F00 * F01 + F10 * F11;
@@ -334,8 +409,8 @@ __device__ __forceinline__ double lmax2(double F00, double F01, double F10, doub
   return (l2 > l1) ? l2 : l1;
 }
 
-__device__ __forceinline__ double lmax3_sym(double a00, double a01, double a02, double a11,
-                                            double a12, double a22) {
+__device__ __noinline__ double lmax3_sym(double a00, double a01, double a02, double a11,
+                                         double a12, double a22) {
   double a[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
   for (int sweep = 0; sweep < 32; ++sweep) {
     const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
@@ -373,19 +448,108 @@ __device__ __forceinline__ double lmax3_sym(double a00, double a01, double a02, 
   return mx;
 }
 
-__device__ __forceinline__ int plus_r(int j) { return j == 0 ? 1 : 2 * j; }
-__device__ __forceinline__ int minus_r(int j) { return j == 0 ? 0 : 2 * j + 1; }
+// Per stage: centroid velocity uc and differences du[k] = u(c + d_k + a*kd_k) - uc.
+template <int DIM, int STORAGE, bool BLEND>
+__device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
+                                           const unsigned char *__restrict__ recs, float alpha,
+                                           const double *cs, const float (*d)[DIM],
+                                           const float (*kd)[DIM], float as, float *uc,
+                                           float (*du)[DIM], float *slots) {
+  constexpr int K = 2 * DIM;
+  constexpr int NC = 1 << DIM;
+  constexpr bool FX = STORAGE == FTLE_FX15;
+  const GridK &g = m.w.g;
+  int ci[DIM];
+  float fc[DIM];
+  bool ok = true;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const double p = fma(cs[a], m.inv_sp[a], -m.org_sp[a]);
+    const double fl = floor(p);
+    ok = ok && fabs(fl) < 1.0e9;
+    ci[a] = ok ? (int)fl : 0;
+    fc[a] = ok ? (float)(p - fl) : 0.0f;
+  }
+  float A[DIM][NC];
+  bool cin;
+  {
+    float v[DIM][NC];
+    cin = ok && cell_values<DIM, STORAGE, BLEND>(g, recs, alpha, ci, v);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) poly_setup<DIM>(v[c], A[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    const float p = poly_eval<DIM>(A[c], fc);
+    uc[c] = cin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
+  }
+  unsigned off = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    float dl[DIM], F[DIM];
+    bool same = true;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      dl[a] = fmaf(as, kd[k][a], d[k][a]) * m.inv_spf[a];
+      F[a] = fc[a] + dl[a];
+      same = same && F[a] >= 0.0f && F[a] < 1.0f;
+    }
+    if (same) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        const float dp = poly_diff<DIM>(A[c], fc, dl, F);
+        du[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
+      }
+    } else {
+      off |= 1u << k;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
+    }
+  }
+  // neighbours outside the centroid's cell: one shared gather path
+  unsigned rem = off;
+  while (rem) {
+    const int k = __ffs(rem) - 1;
+    rem &= rem - 1;
+    float q[DIM];
+    int cell[DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      const float Fa = slots[(k * DIM + a) * kBlock];
+      const float fo = floorf(Fa);
+      cell[a] = ci[a] + (int)fo;
+      q[a] = Fa - fo;
+    }
+    float v[DIM][NC];
+    const bool kin = ok && cell_values<DIM, STORAGE, BLEND>(g, recs, alpha, cell, v);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      const float p = interp_lerp<DIM>(v[c], q);
+      const float u = kin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
+      slots[(k * DIM + c) * kBlock] = u;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (off & (1u << k)) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) du[k][c] = slots[(k * DIM + c) * kBlock] - uc[c];
+    }
+  }
+}
 
-// ---------------------------------------------------------------------------
-// the window kernel: one thread per neighbour group
-// ---------------------------------------------------------------------------
 template <int DIM, int MODE, int INTEG, int STORAGE>
-__global__ void __launch_bounds__(128) window_mixed_kernel(const MixK m) {
+__global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
   constexpr int K = 2 * DIM;
   constexpr bool BLEND = MODE == FTLE_BLEND;
+  __shared__ float smem_slots[K * DIM * kBlock];
+  float *slots = smem_slots + threadIdx.x;
   const long long N = m.w.N;
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= N) return;
+  const long long g = (long long)blockIdx.x * kBlock + threadIdx.x;
+  if (g >= N) return;  // no block-level synchronisation below
+  const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
+  const unsigned char *recs0 = static_cast<const unsigned char *>(m.w.snaps);
+  (void)recs0;
 
   double c[DIM];
   float d[K][DIM];
@@ -413,101 +577,87 @@ __global__ void __launch_bounds__(128) window_mixed_kernel(const MixK m) {
 
   const double h = m.w.h;
   const float hf = (float)h;
-  float ucp[DIM], dup[K][DIM];  // AB2 history
+  float kc[DIM], kd[K][DIM], accc[DIM], accd[K][DIM];
+  float kcp[DIM], kdp[K][DIM];  // AB2 history
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) kc[a] = kcp[a] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) kd[k][a] = kdp[k][a] = 0.0f;
+
+  constexpr int NST = INTEG == FTLE_RK4 ? 4 : 1;
   for (int i = 0; i < m.w.num_steps; ++i) {
     const double t = m.w.t0 + (double)i * h;
-    float uc[DIM], du[K][DIM];
-    float alpha;
-    if constexpr (INTEG == FTLE_EULER || INTEG == FTLE_AB2) {
-      const void *base = record_set<DIM, MODE>(m, i, t, alpha);
-      eval_group<DIM, BLEND, STORAGE>(m, base, alpha, c, d, uc, du);
-      if (INTEG == FTLE_EULER || i == 0) {
+#pragma unroll 1
+    for (int s = 0; s < NST; ++s) {
+      // RK4 tableau: stage point x + a*k_prev, weight w, time t + tc*h
+      const float tc = (s == 0) ? 0.0f : (s == 3 ? 1.0f : 0.5f);
+      const float as = tc * hf;
+      const float ws = (s == 0 || s == 3) ? 1.0f : 2.0f;
+      float alpha;
+      const unsigned char *recs = record_set<DIM, MODE>(m, i, t + (double)tc * h, alpha);
+      double cs[DIM];
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) c[a] += h * (double)uc[a];
+      for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], c[a]);
+      float uc[DIM], du[K][DIM];
+      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, d, kd, as, uc, du, slots);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        kc[a] = uc[a];
+        accc[a] = s == 0 ? uc[a] : fmaf(ws, uc[a], accc[a]);
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+          kd[k][a] = du[k][a];
+          accd[k][a] = s == 0 ? du[k][a] : fmaf(ws, du[k][a], accd[k][a]);
+        }
+    }
+    if constexpr (INTEG == FTLE_RK4) {
+      const double h6 = h / 6.0;
+      const float h6f = (float)h6;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) c[a] = fma(h6, (double)accc[a], c[a]);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(h6f, accd[k][a], d[k][a]);
+    } else if constexpr (INTEG == FTLE_EULER) {
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) c[a] = fma(h, (double)kc[a], c[a]);
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(hf, kd[k][a], d[k][a]);
+    } else {  // AB2, Euler on the first step (integrate.py:240-246)
+      if (i == 0) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) c[a] = fma(h, (double)kc[a], c[a]);
 #pragma unroll
         for (int k = 0; k < K; ++k)
 #pragma unroll
-          for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(hf, du[k][a], d[k][a]);
+          for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(hf, kd[k][a], d[k][a]);
       } else {
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) c[a] += h * (1.5 * (double)uc[a] - 0.5 * (double)ucp[a]);
+        for (int a = 0; a < DIM; ++a)
+          c[a] = fma(h, 1.5 * (double)kc[a] - 0.5 * (double)kcp[a], c[a]);
 #pragma unroll
         for (int k = 0; k < K; ++k)
 #pragma unroll
           for (int a = 0; a < DIM; ++a)
-            d[k][a] = fmaf(hf, fmaf(1.5f, du[k][a], -0.5f * dup[k][a]), d[k][a]);
+            d[k][a] = fmaf(hf, fmaf(1.5f, kd[k][a], -0.5f * kdp[k][a]), d[k][a]);
       }
-      if constexpr (INTEG == FTLE_AB2) {
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) ucp[a] = uc[a];
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-#pragma unroll
-          for (int a = 0; a < DIM; ++a) dup[k][a] = du[k][a];
-      }
-    } else {
-      const double hh = 0.5 * h;
-      const float hhf = (float)hh;
-      double cs[DIM], accc[DIM];
-      float ds[K][DIM], accd[K][DIM];
-      // stage 1
-      const void *b0 = record_set<DIM, MODE>(m, i, t, alpha);
-      eval_group<DIM, BLEND, STORAGE>(m, b0, alpha, c, d, uc, du);
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) {
-        accc[a] = (double)uc[a];
-        cs[a] = c[a] + hh * (double)uc[a];
-      }
+      for (int a = 0; a < DIM; ++a) kcp[a] = kc[a];
 #pragma unroll
       for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-          accd[k][a] = du[k][a];
-          ds[k][a] = fmaf(hhf, du[k][a], d[k][a]);
-        }
-      // stage 2
-      float alpha_h;
-      const void *bh = record_set<DIM, MODE>(m, i, t + hh, alpha_h);
-      eval_group<DIM, BLEND, STORAGE>(m, bh, alpha_h, cs, ds, uc, du);
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) {
-        accc[a] += 2.0 * (double)uc[a];
-        cs[a] = c[a] + hh * (double)uc[a];
-      }
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-          accd[k][a] = fmaf(2.0f, du[k][a], accd[k][a]);
-          ds[k][a] = fmaf(hhf, du[k][a], d[k][a]);
-        }
-      // stage 3
-      eval_group<DIM, BLEND, STORAGE>(m, bh, alpha_h, cs, ds, uc, du);
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) {
-        accc[a] += 2.0 * (double)uc[a];
-        cs[a] = c[a] + h * (double)uc[a];
-      }
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-          accd[k][a] = fmaf(2.0f, du[k][a], accd[k][a]);
-          ds[k][a] = fmaf(hf, du[k][a], d[k][a]);
-        }
-      // stage 4
-      float alpha_f;
-      const void *bf = record_set<DIM, MODE>(m, i, t + h, alpha_f);
-      eval_group<DIM, BLEND, STORAGE>(m, bf, alpha_f, cs, ds, uc, du);
-      const double h6 = h / 6.0;
-      const float h6f = (float)h6;
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) c[a] += h6 * (accc[a] + (double)uc[a]);
-#pragma unroll
-      for (int k = 0; k < K; ++k)
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(h6f, accd[k][a] + du[k][a], d[k][a]);
+        for (int a = 0; a < DIM; ++a) kdp[k][a] = kd[k][a];
     }
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) kc[a] = 0.0f;  // next step's first stage starts at c
   }
 
   // final positions x_k = c + d_k (FP64)
@@ -542,21 +692,23 @@ __global__ void __launch_bounds__(128) window_mixed_kernel(const MixK m) {
 
 template <int DIM, int MODE, int STORAGE>
 static void launch_mixed(const MixK &m, int integ, cudaStream_t st) {
-  const unsigned blocks = (unsigned)((m.w.N + 127) / 128);
+  const unsigned blocks = (unsigned)((m.w.N + kBlock - 1) / kBlock);
   if (integ == FTLE_EULER)
-    window_mixed_kernel<DIM, MODE, FTLE_EULER, STORAGE><<<blocks, 128, 0, st>>>(m);
+    window_mixed_kernel<DIM, MODE, FTLE_EULER, STORAGE><<<blocks, kBlock, 0, st>>>(m);
   else if (integ == FTLE_AB2)
-    window_mixed_kernel<DIM, MODE, FTLE_AB2, STORAGE><<<blocks, 128, 0, st>>>(m);
+    window_mixed_kernel<DIM, MODE, FTLE_AB2, STORAGE><<<blocks, kBlock, 0, st>>>(m);
   else
-    window_mixed_kernel<DIM, MODE, FTLE_RK4, STORAGE><<<blocks, 128, 0, st>>>(m);
+    window_mixed_kernel<DIM, MODE, FTLE_RK4, STORAGE><<<blocks, kBlock, 0, st>>>(m);
 }
 
 template <int DIM, int MODE>
 static void launch_mixed_s(const MixK &m, int integ, int storage, cudaStream_t st) {
   if (storage == FTLE_F16)
     launch_mixed<DIM, MODE, FTLE_F16>(m, integ, st);
-  else
+  else if (storage == FTLE_BF16)
     launch_mixed<DIM, MODE, FTLE_BF16>(m, integ, st);
+  else
+    launch_mixed<DIM, MODE, FTLE_FX15>(m, integ, st);
 }
 
 }  // namespace ftle
@@ -567,11 +719,12 @@ extern "C" int ftle_window_run_mixed(const ftle_window *w, void *stream) {
   MixK m;
   int rc = window_to_kernel(w, &m.w);
   if (rc) return rc;
-  if (w->storage != FTLE_F16 && w->storage != FTLE_BF16)
-    return fail_invalid("ftle_window_run_mixed needs FTLE_F16 or FTLE_BF16 storage");
+  if (w->storage != FTLE_F16 && w->storage != FTLE_BF16 && w->storage != FTLE_FX15)
+    return fail_invalid("ftle_window_run_mixed needs FTLE_F16, FTLE_BF16 or FTLE_FX15 storage");
   if (m.w.N == 0) return FTLE_OK;
   for (int a = 0; a < 3; ++a) {
     m.inv_sp[a] = 1.0 / m.w.g.spacing[a];
+    m.org_sp[a] = m.w.g.origin[a] / m.w.g.spacing[a];
     m.inv_spf[a] = (float)m.inv_sp[a];
   }
   m.inv_dt = 1.0 / (w->snapshot_dt != 0.0 ? w->snapshot_dt : 1.0);

@@ -42,8 +42,9 @@ def test_packed_sizes():
     lib = _lib.load()
     assert lib.ftle_packed_snapshot_bytes(2, 100, 3, _lib.F64) == 100 * 3 * 32
     assert lib.ftle_packed_snapshot_bytes(3, 100, 3, _lib.F64) == 100 * 3 * 48
-    assert lib.ftle_packed_snapshot_bytes(2, 100, 3, _lib.F16) == 100 * 3 * 8
-    assert lib.ftle_packed_snapshot_bytes(3, 100, 3, _lib.BF16) == 100 * 3 * 16
+    assert lib.ftle_packed_snapshot_bytes(2, 100, 3, _lib.F16) == 256 + 100 * 3 * 8
+    assert lib.ftle_packed_snapshot_bytes(3, 100, 3, _lib.BF16) == 256 + 100 * 3 * 16
+    assert lib.ftle_packed_snapshot_bytes(3, 100, 3, _lib.FX15) == 256 + 100 * 3 * 16
     assert lib.ftle_packed_snapshot_bytes(4, 100, 3, _lib.F16) == -1
 
 
