@@ -239,35 +239,55 @@ struct MixK {
   WinK w;
   double inv_sp[3];   // 1/spacing
   double org_sp[3];   // origin/spacing: p = x*inv_sp - org_sp
+  double period[3];   // n*spacing (periodic grids)
   float inv_spf[3];
+  int stride[3];      // node-index stride per axis (2D: 1, nx; 3D: nz, nx*nz, 1)
   double inv_dt;
+  double inv_S;       // 1/num_snapshots
 };
 
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
 
+// Wrap a cell index into [0, n): one conditional step covers every index
+// within one period of the grid (the centroid is kept in the primary period).
+__device__ __forceinline__ int wrap_near(int q, int n) {
+  if (q < 0)
+    q += n;
+  else if (q >= n)
+    q -= n;
+  if ((unsigned)q >= (unsigned)n) q = wrap_index(q, n);
+  return q;
+}
+
 // Time-blended corner values v[c][q] of the cell whose lower corner is `cell`
 // (q = x + 2y (+ 4z)); false if the cell is outside a non-periodic grid.
 template <int DIM, int STORAGE, bool BLEND>
-__device__ __forceinline__ bool cell_values(const GridK &g, const unsigned char *__restrict__ recs,
+__device__ __forceinline__ bool cell_values(const MixK &m, const unsigned char *__restrict__ recs,
                                             float alpha, const int *cell, float (*v)[1 << DIM]) {
-  int lo[DIM], hi[DIM];
+  const GridK &g = m.w.g;
+  int base = 0, step[DIM];
 #pragma unroll
   for (int a = 0; a < DIM; ++a) {
+    int lo = cell[a];
+    step[a] = m.stride[a];
     if (g.periodic) {
-      lo[a] = wrap_index(cell[a], g.n[a]);
-      hi[a] = lo[a] + 1 == g.n[a] ? 0 : lo[a] + 1;
-    } else {
-      if (cell[a] < 0 || cell[a] > g.n[a] - 2) return false;
-      lo[a] = cell[a];
-      hi[a] = cell[a] + 1;
+      lo = wrap_near(lo, g.n[a]);
+      if (lo + 1 == g.n[a]) step[a] = -(g.n[a] - 1) * m.stride[a];
+    } else if (lo < 0 || lo > g.n[a] - 2) {
+      return false;
     }
+    base += lo * m.stride[a];
   }
 #pragma unroll
   for (int q = 0; q < (1 << DIM); ++q) {
-    const int i = (q & 1) ? hi[0] : lo[0];
-    const int j = (q & 2) ? hi[1] : lo[1];
+    int idx = base;
+    if (q & 1) idx += step[0];
+    if (q & 2) idx += step[1];
+    if constexpr (DIM == 3) {
+      if (q & 4) idx += step[2];
+    }
     if constexpr (DIM == 2) {
-      const uint2 r = __ldg(reinterpret_cast<const uint2 *>(recs) + node2(g, i, j));
+      const uint2 r = __ldg(reinterpret_cast<const uint2 *>(recs) + idx);
       const float u0 = Dec<STORAGE>::lo(r.x), v0 = Dec<STORAGE>::hi(r.x);
       if constexpr (BLEND) {
         v[0][q] = lerpf(u0, Dec<STORAGE>::lo(r.y), alpha);
@@ -277,8 +297,7 @@ __device__ __forceinline__ bool cell_values(const GridK &g, const unsigned char 
         v[1][q] = v0;
       }
     } else {
-      const int k = (q & 4) ? hi[2] : lo[2];
-      const uint4 r = __ldg(reinterpret_cast<const uint4 *>(recs) + node3(g, i, j, k));
+      const uint4 r = __ldg(reinterpret_cast<const uint4 *>(recs) + idx);
       const float u0 = Dec<STORAGE>::lo(r.x), v0 = Dec<STORAGE>::hi(r.x);
       const float w0 = Dec<STORAGE>::lo(r.y);
       if constexpr (BLEND) {
@@ -375,7 +394,7 @@ __device__ __forceinline__ const unsigned char *record_set(const MixK &m, int st
     double tau = (t - m.w.snap_t0) * m.inv_dt;
     const int S = m.w.num_snaps;
     if (m.w.periodic_time) {
-      tau = tau - (double)S * floor(tau / (double)S);
+      tau = tau - (double)S * floor(tau * m.inv_S);
       s = (int)floor(tau);
       s = s >= S ? S - 1 : (s < 0 ? 0 : s);
       alpha = (float)(tau - (double)s);
@@ -448,17 +467,29 @@ __device__ __noinline__ double lmax3_sym(double a00, double a01, double a02, dou
   return mx;
 }
 
+// Off-cell neighbour work items of one warp (structure of arrays, per warp).
+template <int DIM>
+struct WarpQueue {
+  static constexpr int kCap = 32 * 2 * DIM;
+  int cell[DIM][kCap];
+  float q[DIM][kCap];
+  int dst[kCap];  // slot index of the owning thread's neighbour
+};
+
 // Per stage: centroid velocity uc and differences du[k] = u(c + d_k + a*kd_k) - uc.
+// Neighbours inside the centroid's cell use the cell polynomial; the others are
+// queued per warp and gathered 32 at a time, so no lane idles in a divergent loop.
 template <int DIM, int STORAGE, bool BLEND>
 __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
                                            const unsigned char *__restrict__ recs, float alpha,
                                            const double *cs, const float (*d)[DIM],
                                            const float (*kd)[DIM], float as, float *uc,
-                                           float (*du)[DIM], float *slots) {
+                                           float (*du)[DIM], float *slots_base,
+                                           WarpQueue<DIM> &wq, int lane) {
   constexpr int K = 2 * DIM;
   constexpr int NC = 1 << DIM;
   constexpr bool FX = STORAGE == FTLE_FX15;
-  const GridK &g = m.w.g;
+  float *slots = slots_base + threadIdx.x;
   int ci[DIM];
   float fc[DIM];
   bool ok = true;
@@ -474,7 +505,7 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
   bool cin;
   {
     float v[DIM][NC];
-    cin = ok && cell_values<DIM, STORAGE, BLEND>(g, recs, alpha, ci, v);
+    cin = ok && cell_values<DIM, STORAGE, BLEND>(m, recs, alpha, ci, v);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) poly_setup<DIM>(v[c], A[c]);
   }
@@ -483,6 +514,7 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
     const float p = poly_eval<DIM>(A[c], fc);
     uc[c] = cin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
   }
+  // pass 1: every neighbour through the cell polynomial; flag those outside the cell
   unsigned off = 0;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
@@ -494,41 +526,62 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
       F[a] = fc[a] + dl[a];
       same = same && F[a] >= 0.0f && F[a] < 1.0f;
     }
-    if (same) {
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        const float dp = poly_diff<DIM>(A[c], fc, dl, F);
-        du[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
-      }
-    } else {
-      off |= 1u << k;
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
-    }
-  }
-  // neighbours outside the centroid's cell: one shared gather path
-  unsigned rem = off;
-  while (rem) {
-    const int k = __ffs(rem) - 1;
-    rem &= rem - 1;
-    float q[DIM];
-    int cell[DIM];
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-      const float Fa = slots[(k * DIM + a) * kBlock];
-      const float fo = floorf(Fa);
-      cell[a] = ci[a] + (int)fo;
-      q[a] = Fa - fo;
-    }
-    float v[DIM][NC];
-    const bool kin = ok && cell_values<DIM, STORAGE, BLEND>(g, recs, alpha, cell, v);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      const float p = interp_lerp<DIM>(v[c], q);
-      const float u = kin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
-      slots[(k * DIM + c) * kBlock] = u;
+      const float dp = poly_diff<DIM>(A[c], fc, dl, F);
+      du[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
+    }
+    off |= same ? 0u : (1u << k);
+  }
+  // pass 2: queue the off-cell neighbours of the whole warp
+  const int cnt = __popc(off);
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0) return;  // warp-uniform
+  __syncwarp();  // every lane has read its slots of the previous stage
+  int pos = incl - cnt;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (off & (1u << k)) {
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        const float F = fmaf(fmaf(as, kd[k][a], d[k][a]), m.inv_spf[a], fc[a]);
+        const float fo = floorf(F);
+        wq.cell[a][pos] = ci[a] + (int)fo;
+        wq.q[a][pos] = F - fo;
+      }
+      wq.dst[pos] = k * DIM * kBlock + (int)threadIdx.x;
+      ++pos;
     }
   }
+  __syncwarp();
+  // pass 3: 32 queued gathers at a time
+  for (int b = 0; b < total; b += 32) {
+    const int it = b + lane;
+    if (it < total) {
+      int cell[DIM];
+      float q[DIM];
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        cell[a] = wq.cell[a][it];
+        q[a] = wq.q[a][it];
+      }
+      float v[DIM][NC];
+      const bool kin = ok && cell_values<DIM, STORAGE, BLEND>(m, recs, alpha, cell, v);
+      const int dst = wq.dst[it];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        const float p = interp_lerp<DIM>(v[c], q);
+        slots_base[dst + c * kBlock] = kin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
+      }
+    }
+  }
+  __syncwarp();
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     if (off & (1u << k)) {
@@ -543,15 +596,19 @@ __global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
   constexpr int K = 2 * DIM;
   constexpr bool BLEND = MODE == FTLE_BLEND;
   __shared__ float smem_slots[K * DIM * kBlock];
-  float *slots = smem_slots + threadIdx.x;
+  __shared__ WarpQueue<DIM> smem_queue[kBlock / 32];
+  const int lane = threadIdx.x & 31;
+  WarpQueue<DIM> &wq = smem_queue[threadIdx.x >> 5];
   const long long N = m.w.N;
-  const long long g = (long long)blockIdx.x * kBlock + threadIdx.x;
-  if (g >= N) return;  // no block-level synchronisation below
+  const long long g_raw = (long long)blockIdx.x * kBlock + threadIdx.x;
+  // lanes past the end mirror the last group (warp-wide shuffles need every lane) but write nothing
+  const bool active = g_raw < N;
+  const long long g = active ? g_raw : N - 1;
   const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
-  const unsigned char *recs0 = static_cast<const unsigned char *>(m.w.snaps);
-  (void)recs0;
+  const bool periodic = m.w.g.periodic != 0;
 
   double c[DIM];
+  int wraps[DIM];
   float d[K][DIM];
   double id[DIM];
   {
@@ -573,6 +630,18 @@ __global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
       for (int a = 0; a < DIM; ++a) d[k][a] = (float)(X[k][a] - c[a]);
 #pragma unroll
     for (int j = 0; j < DIM; ++j) id[j] = X[plus_r(j)][j] - X[minus_r(j)][j];
+  }
+  // periodic grids: keep the centroid in the primary period, count the wraps
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    wraps[a] = 0;
+    if (periodic) {
+      const double w = floor((c[a] - m.w.g.origin[a]) / m.period[a]);
+      if (fabs(w) < 1.0e9) {
+        wraps[a] = (int)w;
+        c[a] -= w * m.period[a];
+      }
+    }
   }
 
   const double h = m.w.h;
@@ -601,7 +670,8 @@ __global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
 #pragma unroll
       for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], c[a]);
       float uc[DIM], du[K][DIM];
-      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, d, kd, as, uc, du, slots);
+      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, d, kd, as, uc, du, smem_slots, wq,
+                                      lane);
 #pragma unroll
       for (int a = 0; a < DIM; ++a) {
         kc[a] = uc[a];
@@ -657,10 +727,26 @@ __global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
         for (int a = 0; a < DIM; ++a) kdp[k][a] = kd[k][a];
     }
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) kc[a] = 0.0f;  // next step's first stage starts at c
+    for (int a = 0; a < DIM; ++a) {
+      kc[a] = 0.0f;  // next step's first stage starts at c
+      if (periodic) {  // one period at most per step
+        const double lo = m.w.g.origin[a], hi = lo + m.period[a];
+        if (c[a] < lo) {
+          c[a] += m.period[a];
+          --wraps[a];
+        } else if (c[a] >= hi) {
+          c[a] -= m.period[a];
+          ++wraps[a];
+        }
+      }
+    }
   }
+  if (!active) return;
 
-  // final positions x_k = c + d_k (FP64)
+  // final positions x_k = c + wraps*period + d_k (FP64)
+#pragma unroll
+  for (int a = 0; a < DIM; ++a)
+    if (periodic) c[a] += (double)wraps[a] * m.period[a];
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -722,12 +808,25 @@ extern "C" int ftle_window_run_mixed(const ftle_window *w, void *stream) {
   if (w->storage != FTLE_F16 && w->storage != FTLE_BF16 && w->storage != FTLE_FX15)
     return fail_invalid("ftle_window_run_mixed needs FTLE_F16, FTLE_BF16 or FTLE_FX15 storage");
   if (m.w.N == 0) return FTLE_OK;
+  if (m.w.g.nodes >= (1LL << 31))
+    return fail_invalid("the mixed-precision window supports grids below 2^31 nodes");
   for (int a = 0; a < 3; ++a) {
     m.inv_sp[a] = 1.0 / m.w.g.spacing[a];
     m.org_sp[a] = m.w.g.origin[a] / m.w.g.spacing[a];
     m.inv_spf[a] = (float)m.inv_sp[a];
+    m.period[a] = (double)m.w.g.n[a] * m.w.g.spacing[a];
+  }
+  if (w->grid.dim == 2) {
+    m.stride[0] = 1;
+    m.stride[1] = m.w.g.n[0];
+    m.stride[2] = 0;
+  } else {
+    m.stride[0] = m.w.g.n[2];
+    m.stride[1] = m.w.g.n[0] * m.w.g.n[2];
+    m.stride[2] = 1;
   }
   m.inv_dt = 1.0 / (w->snapshot_dt != 0.0 ? w->snapshot_dt : 1.0);
+  m.inv_S = 1.0 / (double)m.w.num_snaps;
   cudaStream_t st = as_stream(stream);
   if (w->grid.dim == 2) {
     if (w->time_mode == FTLE_HOLD)
