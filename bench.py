@@ -55,6 +55,9 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
     p.add_argument("--h", type=float, default=0.02)
     p.add_argument("--T", type=float, default=8.0)
+    p.add_argument("--chunk-steps", type=int, default=50,
+                   help="mixed path: steps per launch between cell sorts (0: one launch)")
+    p.add_argument("--sort-every", type=int, default=1)
     p.add_argument("--plain-fraction", type=float, default=0.125,
                    help="share of the groups the plain FP64 leg advects")
     p.add_argument("--no-plain", action="store_true")
@@ -271,11 +274,23 @@ def run_ours(args):
     series = SnapshotSeries(grid, snaps_d, precision=args.precision, periodic_time=True)
     kw = dict(integrator="rk4", time_mode="blend", h=w["h"], num_steps=w["num_steps"],
               map_period=w["num_steps"] * w["h"], t0=t0, snapshot_dt=w["snap_dt"])
+    chunk = args.chunk_steps if (args.chunk_steps > 0 and args.precision != "fp64") else None
+    kw_chosen = dict(kw, chunk_steps=chunk, sort_every=args.sort_every)
+    workspace = None
+    if chunk is not None:
+        from pyftle_b200 import _lib as _l
+        from pyftle_b200.window import window_descriptor
+
+        need = _l.load().ftle_window_workspace_bytes(window_descriptor(
+            series, pos0, None, integrator="rk4", time_mode="blend", h=w["h"],
+            num_steps=w["num_steps"], map_period=1.0))
+        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+    kw_chosen["workspace"] = workspace
     stream = torch.cuda.current_stream()
 
     def one_window(out=None):
         pos.copy_(pos0)
-        return run_window(series, pos, ftle_out=ftle if out is None else out, **kw)
+        return run_window(series, pos, ftle_out=ftle if out is None else out, **kw_chosen)
 
     for _ in range(args.warmup):
         one_window()
@@ -293,7 +308,7 @@ def run_ours(args):
     for k in range(args.steps):
         pos.copy_(pos0)
         k_start[k].record(stream)
-        run_window(series, pos, ftle_out=ftle, **kw)
+        run_window(series, pos, ftle_out=ftle, **kw_chosen)
         k_end[k].record(stream)
     ev_end.record(stream)
     torch.cuda.synchronize()
@@ -347,7 +362,8 @@ def run_ours(args):
         h2d = snaps_pin.numel() * 8 + pos_pin.numel() * 8
         d2h = N * 8
         integ = create_integrator("rk4", create_interpolator("grid", (n, n, n), periodic=True))
-        opts = EngineOptions(precision=args.precision)
+        opts = EngineOptions(precision=args.precision, chunk_steps=chunk,
+                             sort_every=args.sort_every)
 
         def e2e_step():
             src = BlendedSnapshotSource(snaps_pin, pts, pos_pin, (n, n, n), h=w["h"],
@@ -373,6 +389,14 @@ def run_ours(args):
                "path": "FTLESolver.run(BlendedSnapshotSource(pinned host arrays))"}
         assert np.isfinite(field).all()
         del snaps_pin, pos_pin
+
+    # our kernels per window: one launch per chunk, plus 3 sort kernels per sorted boundary
+    if chunk is None:
+        launches_per_window = 1
+    else:
+        nch = -(-w["num_steps"] // chunk)
+        nsort = sum(1 for ci in range(nch - 1) if args.sort_every > 0 and (ci + 1) % args.sort_every == 0)
+        launches_per_window = nch + 3 * nsort
 
     # --- roofline of the dominant kernel --------------------------------------
     peaks = {}
@@ -413,12 +437,13 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if elem == 2 else "f64", "data": "synthetic",
             "config": {"workload": workload_name(w), "precision": args.precision,
+                       "chunk_steps": chunk, "sort_every": args.sort_every,
                        "particles": K * N, "groups": N, "rk4_steps": w["num_steps"],
                        "particle_steps_per_window": particle_steps,
                        "l2": "inputs larger than L2 (positions 2.4 GB, packed snapshots)",
                        "rank_windows": "rank r starts at t0 = r * snapshot_dt"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": args.steps, "clocks": clk, "plain_fp64": plain,
+            "gpu_launches": args.steps * launches_per_window, "clocks": clk, "plain_fp64": plain,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

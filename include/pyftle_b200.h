@@ -167,6 +167,21 @@ int ftle_window_run_f64(const ftle_window *w, void *stream);
  * FP64 positions = centroid + offset. */
 int ftle_window_run_mixed(const ftle_window *w, void *stream);
 
+/* Bytes of device workspace ftle_window_run_mixed_chunked needs for `w`
+ * (two group-state buffers, sort keys and bins); -1 for an invalid descriptor. */
+int64_t ftle_window_workspace_bytes(const ftle_window *w);
+
+/* The mixed-precision window in launches of `chunk_steps` steps: between
+ * launches each group's state (FP64 centroid, FP32 offsets) lives in the
+ * caller's `workspace` (256-byte aligned, >= ftle_window_workspace_bytes),
+ * and every `sort_every` chunks (0 = never) the groups are reordered by the
+ * Morton code of their centroid's cell, so that each block advects
+ * neighbouring groups and their gathers share cached snapshot records.
+ * Per-group arithmetic is unchanged: results equal ftle_window_run_mixed. */
+int ftle_window_run_mixed_chunked(const ftle_window *w, void *workspace,
+                                  int64_t workspace_bytes, int32_t chunk_steps,
+                                  int32_t sort_every, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

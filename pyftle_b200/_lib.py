@@ -69,6 +69,9 @@ SIGNATURES = {
     "ftle_pack_snapshots": (ctypes.c_int, [_i32, _i64, _i32, _i32, _c_dp, _i32, _c_dp, _c_dp]),
     "ftle_window_run_f64": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp]),
     "ftle_window_run_mixed": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp]),
+    "ftle_window_workspace_bytes": (ctypes.c_int64, [ctypes.POINTER(FtleWindow)]),
+    "ftle_window_run_mixed_chunked": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp, _i64,
+                                                     _i32, _i32, _c_dp]),
 }
 
 _lock = threading.Lock()

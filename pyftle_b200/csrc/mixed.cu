@@ -476,16 +476,16 @@ struct WarpQueue {
   int dst[kCap];  // slot index of the owning thread's neighbour
 };
 
-// Per stage: centroid velocity uc and differences du[k] = u(c + d_k + a*kd_k) - uc.
+// Per stage: centroid velocity uc and, in place of the previous stage's kd[k], the
+// differences kd[k] = u(c + d_k + a*kd_k) - uc.
 // Neighbours inside the centroid's cell use the cell polynomial; the others are
 // queued per warp and gathered 32 at a time, so no lane idles in a divergent loop.
 template <int DIM, int STORAGE, bool BLEND>
 __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
                                            const unsigned char *__restrict__ recs, float alpha,
                                            const double *cs, const float (*d)[DIM],
-                                           const float (*kd)[DIM], float as, float *uc,
-                                           float (*du)[DIM], float *slots_base,
-                                           WarpQueue<DIM> &wq, int lane) {
+                                           float (*kd)[DIM], float as, float *uc,
+                                           float *slots_base, WarpQueue<DIM> &wq, int lane) {
   constexpr int K = 2 * DIM;
   constexpr int NC = 1 << DIM;
   constexpr bool FX = STORAGE == FTLE_FX15;
@@ -529,9 +529,13 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
       const float dp = poly_diff<DIM>(A[c], fc, dl, F);
-      du[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
+      kd[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
     }
-    off |= same ? 0u : (1u << k);
+    if (!same) {
+      off |= 1u << k;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
+    }
   }
   // pass 2: queue the off-cell neighbours of the whole warp
   const int cnt = __popc(off);
@@ -550,7 +554,7 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
     if (off & (1u << k)) {
 #pragma unroll
       for (int a = 0; a < DIM; ++a) {
-        const float F = fmaf(fmaf(as, kd[k][a], d[k][a]), m.inv_spf[a], fc[a]);
+        const float F = slots[(k * DIM + a) * kBlock];
         const float fo = floorf(F);
         wq.cell[a][pos] = ci[a] + (int)fo;
         wq.q[a][pos] = F - fo;
@@ -586,77 +590,87 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
   for (int k = 0; k < K; ++k) {
     if (off & (1u << k)) {
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) du[k][c] = slots[(k * DIM + c) * kBlock] - uc[c];
+      for (int c = 0; c < DIM; ++c) kd[k][c] = slots[(k * DIM + c) * kBlock] - uc[c];
     }
   }
 }
 
-template <int DIM, int MODE, int INTEG, int STORAGE>
-__global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
+// ---------------------------------------------------------------------------
+// per-group state and the step loop
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+struct GroupState {
+  double c[DIM];            // centroid (periodic grids: inside the primary period)
+  int wraps[DIM];           // periods removed from the centroid
+  float d[2 * DIM][DIM];    // neighbour offsets
+  double id[DIM];           // initial diagonal separations (Jacobian denominators)
+  float kcp[DIM];           // AB2: previous centroid velocity
+  float kdp[2 * DIM][DIM];  // AB2: previous velocity differences
+};
+
+// Centroid = mean of the K neighbours (particles.py:235-236); offsets relative to it.
+template <int DIM>
+__device__ __forceinline__ void group_from_positions(const MixK &m, long long g,
+                                                     GroupState<DIM> &st) {
   constexpr int K = 2 * DIM;
-  constexpr bool BLEND = MODE == FTLE_BLEND;
-  __shared__ float smem_slots[K * DIM * kBlock];
-  __shared__ WarpQueue<DIM> smem_queue[kBlock / 32];
-  const int lane = threadIdx.x & 31;
-  WarpQueue<DIM> &wq = smem_queue[threadIdx.x >> 5];
   const long long N = m.w.N;
-  const long long g_raw = (long long)blockIdx.x * kBlock + threadIdx.x;
-  // lanes past the end mirror the last group (warp-wide shuffles need every lane) but write nothing
-  const bool active = g_raw < N;
-  const long long g = active ? g_raw : N - 1;
-  const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
-  const bool periodic = m.w.g.periodic != 0;
-
-  double c[DIM];
-  int wraps[DIM];
-  float d[K][DIM];
-  double id[DIM];
-  {
-    double X[K][DIM];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) X[k][a] = m.w.positions[((long long)k * N + g) * DIM + a];
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-      double s = X[0][a];
-#pragma unroll
-      for (int k = 1; k < K; ++k) s += X[k][a];
-      c[a] = s / (double)K;  // particles.py:235-236 (mean of the neighbours)
-    }
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int a = 0; a < DIM; ++a) d[k][a] = (float)(X[k][a] - c[a]);
-#pragma unroll
-    for (int j = 0; j < DIM; ++j) id[j] = X[plus_r(j)][j] - X[minus_r(j)][j];
-  }
-  // periodic grids: keep the centroid in the primary period, count the wraps
-#pragma unroll
-  for (int a = 0; a < DIM; ++a) {
-    wraps[a] = 0;
-    if (periodic) {
-      const double w = floor((c[a] - m.w.g.origin[a]) / m.period[a]);
-      if (fabs(w) < 1.0e9) {
-        wraps[a] = (int)w;
-        c[a] -= w * m.period[a];
-      }
-    }
-  }
-
-  const double h = m.w.h;
-  const float hf = (float)h;
-  float kc[DIM], kd[K][DIM], accc[DIM], accd[K][DIM];
-  float kcp[DIM], kdp[K][DIM];  // AB2 history
-#pragma unroll
-  for (int a = 0; a < DIM; ++a) kc[a] = kcp[a] = 0.0f;
+  double X[K][DIM];
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) kd[k][a] = kdp[k][a] = 0.0f;
+    for (int a = 0; a < DIM; ++a) X[k][a] = m.w.positions[((long long)k * N + g) * DIM + a];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    double s = X[0][a];
+#pragma unroll
+    for (int k = 1; k < K; ++k) s += X[k][a];
+    st.c[a] = s / (double)K;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      st.d[k][a] = (float)(X[k][a] - st.c[a]);
+      st.kdp[k][a] = 0.0f;
+    }
+#pragma unroll
+  for (int j = 0; j < DIM; ++j) st.id[j] = X[plus_r(j)][j] - X[minus_r(j)][j];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    st.kcp[a] = 0.0f;
+    st.wraps[a] = 0;
+    if (m.w.g.periodic) {
+      const double w = floor((st.c[a] - m.w.g.origin[a]) / m.period[a]);
+      if (fabs(w) < 1.0e9) {
+        st.wraps[a] = (int)w;
+        st.c[a] -= w * m.period[a];
+      }
+    }
+  }
+}
+
+// Advect one group through steps [i0, i1) of the window.
+template <int DIM, int MODE, int INTEG, int STORAGE>
+__device__ __forceinline__ void group_advect(const MixK &m, const Header16 &hd,
+                                             GroupState<DIM> &st, int i0, int i1,
+                                             float *smem_slots, float *acc, WarpQueue<DIM> &wq,
+                                             int lane) {
+  constexpr int K = 2 * DIM;
+  constexpr bool BLEND = MODE == FTLE_BLEND;
+  const bool periodic = m.w.g.periodic != 0;
+  const double h = m.w.h;
+  const float hf = (float)h;
+  float kc[DIM], kd[K][DIM], accc[DIM];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) kc[a] = 0.0f;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) kd[k][a] = 0.0f;
 
   constexpr int NST = INTEG == FTLE_RK4 ? 4 : 1;
-  for (int i = 0; i < m.w.num_steps; ++i) {
+  for (int i = i0; i < i1; ++i) {
     const double t = m.w.t0 + (double)i * h;
 #pragma unroll 1
     for (int s = 0; s < NST; ++s) {
@@ -668,98 +682,105 @@ __global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
       const unsigned char *recs = record_set<DIM, MODE>(m, i, t + (double)tc * h, alpha);
       double cs[DIM];
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], c[a]);
-      float uc[DIM], du[K][DIM];
-      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, d, kd, as, uc, du, smem_slots, wq,
+      for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], st.c[a]);
+      float uc[DIM];
+      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, st.d, kd, as, uc, smem_slots, wq,
                                       lane);
 #pragma unroll
       for (int a = 0; a < DIM; ++a) {
         kc[a] = uc[a];
         accc[a] = s == 0 ? uc[a] : fmaf(ws, uc[a], accc[a]);
       }
+      if constexpr (INTEG == FTLE_RK4) {
 #pragma unroll
-      for (int k = 0; k < K; ++k)
+        for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-          kd[k][a] = du[k][a];
-          accd[k][a] = s == 0 ? du[k][a] : fmaf(ws, du[k][a], accd[k][a]);
-        }
+          for (int a = 0; a < DIM; ++a) {
+            float &r = acc[(k * DIM + a) * kBlock];
+            r = s == 0 ? kd[k][a] : fmaf(ws, kd[k][a], r);
+          }
+      }
     }
     if constexpr (INTEG == FTLE_RK4) {
       const double h6 = h / 6.0;
       const float h6f = (float)h6;
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) c[a] = fma(h6, (double)accc[a], c[a]);
+      for (int a = 0; a < DIM; ++a) st.c[a] = fma(h6, (double)accc[a], st.c[a]);
 #pragma unroll
       for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(h6f, accd[k][a], d[k][a]);
+        for (int a = 0; a < DIM; ++a)
+          st.d[k][a] = fmaf(h6f, acc[(k * DIM + a) * kBlock], st.d[k][a]);
     } else if constexpr (INTEG == FTLE_EULER) {
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) c[a] = fma(h, (double)kc[a], c[a]);
+      for (int a = 0; a < DIM; ++a) st.c[a] = fma(h, (double)kc[a], st.c[a]);
 #pragma unroll
       for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(hf, kd[k][a], d[k][a]);
+        for (int a = 0; a < DIM; ++a) st.d[k][a] = fmaf(hf, kd[k][a], st.d[k][a]);
     } else {  // AB2, Euler on the first step (integrate.py:240-246)
       if (i == 0) {
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) c[a] = fma(h, (double)kc[a], c[a]);
+        for (int a = 0; a < DIM; ++a) st.c[a] = fma(h, (double)kc[a], st.c[a]);
 #pragma unroll
         for (int k = 0; k < K; ++k)
 #pragma unroll
-          for (int a = 0; a < DIM; ++a) d[k][a] = fmaf(hf, kd[k][a], d[k][a]);
+          for (int a = 0; a < DIM; ++a) st.d[k][a] = fmaf(hf, kd[k][a], st.d[k][a]);
       } else {
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
-          c[a] = fma(h, 1.5 * (double)kc[a] - 0.5 * (double)kcp[a], c[a]);
+          st.c[a] = fma(h, 1.5 * (double)kc[a] - 0.5 * (double)st.kcp[a], st.c[a]);
 #pragma unroll
         for (int k = 0; k < K; ++k)
 #pragma unroll
           for (int a = 0; a < DIM; ++a)
-            d[k][a] = fmaf(hf, fmaf(1.5f, kd[k][a], -0.5f * kdp[k][a]), d[k][a]);
+            st.d[k][a] = fmaf(hf, fmaf(1.5f, kd[k][a], -0.5f * st.kdp[k][a]), st.d[k][a]);
       }
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) kcp[a] = kc[a];
+      for (int a = 0; a < DIM; ++a) st.kcp[a] = kc[a];
 #pragma unroll
       for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) kdp[k][a] = kd[k][a];
+        for (int a = 0; a < DIM; ++a) st.kdp[k][a] = kd[k][a];
     }
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
       kc[a] = 0.0f;  // next step's first stage starts at c
       if (periodic) {  // one period at most per step
         const double lo = m.w.g.origin[a], hi = lo + m.period[a];
-        if (c[a] < lo) {
-          c[a] += m.period[a];
-          --wraps[a];
-        } else if (c[a] >= hi) {
-          c[a] -= m.period[a];
-          ++wraps[a];
+        if (st.c[a] < lo) {
+          st.c[a] += m.period[a];
+          --st.wraps[a];
+        } else if (st.c[a] >= hi) {
+          st.c[a] -= m.period[a];
+          ++st.wraps[a];
         }
       }
     }
   }
-  if (!active) return;
+}
 
-  // final positions x_k = c + wraps*period + d_k (FP64)
+// Final positions x_k = c + wraps*period + d_k and the FP64 FTLE epilogue.
+template <int DIM>
+__device__ __forceinline__ void group_finish(const MixK &m, long long g, GroupState<DIM> &st) {
+  constexpr int K = 2 * DIM;
+  const long long N = m.w.N;
+  double c[DIM];
 #pragma unroll
   for (int a = 0; a < DIM; ++a)
-    if (periodic) c[a] += (double)wraps[a] * m.period[a];
+    c[a] = m.w.g.periodic ? st.c[a] + (double)st.wraps[a] * m.period[a] : st.c[a];
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
-      m.w.positions[((long long)k * N + g) * DIM + a] = c[a] + (double)d[k][a];
-
+      m.w.positions[((long long)k * N + g) * DIM + a] = c[a] + (double)st.d[k][a];
   if (m.w.ftle != nullptr) {
     double J[DIM][DIM];
 #pragma unroll
     for (int i = 0; i < DIM; ++i)
 #pragma unroll
       for (int j = 0; j < DIM; ++j)
-        J[i][j] = ((double)d[plus_r(j)][i] - (double)d[minus_r(j)][i]) / id[j];
+        J[i][j] = ((double)st.d[plus_r(j)][i] - (double)st.d[minus_r(j)][i]) / st.id[j];
     double lam;
     if constexpr (DIM == 2) {
       lam = lmax2(J[0][0], J[0][1], J[1][0], J[1][1]);
@@ -776,38 +797,229 @@ __global__ void __launch_bounds__(kBlock, 3) window_mixed_kernel(const MixK m) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// chunk state (structure of arrays over N slots) and cell sort
+// ---------------------------------------------------------------------------
+
+struct ChunkBuf {
+  double *c;      // DIM x N
+  int *wraps;     // DIM x N
+  float *d;       // K*DIM x N
+  double *id;     // DIM x N
+  float *hist;    // (DIM + K*DIM) x N, AB2 only
+  long long *idx; // N: original group index
+};
+
+template <int DIM>
+__device__ __forceinline__ void state_load(const ChunkBuf &b, long long N, long long j,
+                                           GroupState<DIM> &st, bool ab2) {
+  constexpr int K = 2 * DIM;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    st.c[a] = b.c[a * N + j];
+    st.wraps[a] = b.wraps[a * N + j];
+    st.id[a] = b.id[a * N + j];
+    st.kcp[a] = ab2 ? b.hist[a * N + j] : 0.0f;
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      st.d[k][a] = b.d[(k * DIM + a) * N + j];
+      st.kdp[k][a] = ab2 ? b.hist[(DIM + k * DIM + a) * N + j] : 0.0f;
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ void state_store(const ChunkBuf &b, long long N, long long j,
+                                            const GroupState<DIM> &st, bool ab2) {
+  constexpr int K = 2 * DIM;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    b.c[a * N + j] = st.c[a];
+    b.wraps[a * N + j] = st.wraps[a];
+    b.id[a * N + j] = st.id[a];
+    if (ab2) b.hist[a * N + j] = st.kcp[a];
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      b.d[(k * DIM + a) * N + j] = st.d[k][a];
+      if (ab2) b.hist[(DIM + k * DIM + a) * N + j] = st.kdp[k][a];
+    }
+}
+
+// Interleave the low `bits` bits of x with stride dim (bits*dim <= 30).
+__device__ __forceinline__ unsigned spread_bits(unsigned x, int dim, int bits) {
+  unsigned r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((x >> b) & 1u) << (b * dim);
+  return r;
+}
+
+// Morton key of the coarse cell holding the centroid (2^bits cells per axis).
+template <int DIM>
+__device__ __forceinline__ int cell_key(const MixK &m, const GroupState<DIM> &st, int bits) {
+  unsigned key = 0;
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) {
+    const double p = fma(st.c[a], m.inv_sp[a], -m.org_sp[a]);
+    const int n = m.w.g.n[a];
+    double fl = floor(p);
+    fl = fl < 0.0 ? 0.0 : (fl > (double)(n - 1) ? (double)(n - 1) : fl);  // NaN -> n-1 side
+    if (!(fl >= 0.0)) fl = 0.0;
+    const unsigned cc = (unsigned)(((long long)fl << bits) / n);
+    key |= spread_bits(cc, DIM, bits) << a;
+  }
+  return (int)(key & ((1u << (bits * DIM)) - 1u));  // always a valid bin
+}
+
+__global__ void sort_hist_kernel(const int *__restrict__ keys, long long N, int *hist) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < N;
+       j += (long long)gridDim.x * blockDim.x)
+    atomicAdd(hist + keys[j], 1);
+}
+
+// in-place exclusive scan of nbins counters (one block of 1024 threads)
+__global__ void sort_scan_kernel(int *bins, int nbins) {
+  __shared__ int part[1024];
+  const int per = (nbins + 1023) / 1024;
+  const int b0 = threadIdx.x * per;
+  int s = 0;
+  for (int i = 0; i < per; ++i)
+    if (b0 + i < nbins) s += bins[b0 + i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - s;  // exclusive prefix of this thread's bins
+  for (int i = 0; i < per; ++i)
+    if (b0 + i < nbins) {
+      const int c = bins[b0 + i];
+      bins[b0 + i] = run;
+      run += c;
+    }
+}
+
+template <int DIM>
+__global__ void sort_scatter_kernel(const int *__restrict__ keys, long long N, int *cursor,
+                                    ChunkBuf in, ChunkBuf out, int ab2) {
+  constexpr int K = 2 * DIM;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < N;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long p = atomicAdd(cursor + keys[j], 1);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      out.c[a * N + p] = in.c[a * N + j];
+      out.wraps[a * N + p] = in.wraps[a * N + j];
+      out.id[a * N + p] = in.id[a * N + j];
+    }
+#pragma unroll
+    for (int q = 0; q < K * DIM; ++q) out.d[q * N + p] = in.d[q * N + j];
+    if (ab2)
+      for (int q = 0; q < DIM + K * DIM; ++q) out.hist[q * N + p] = in.hist[q * N + j];
+    out.idx[p] = in.idx[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// window kernels
+// ---------------------------------------------------------------------------
+
+// One launch advances every group through steps [i0, i1).  first: the state
+// comes from the role-blocked positions (slot = group index); last: final
+// positions and FTLE are written at the group's original index; otherwise
+// the state goes back to `buf` (and its cell key to `keys` when given).
+template <int DIM, int MODE, int INTEG, int STORAGE>
+__global__ void __launch_bounds__(kBlock, 3)
+    window_mixed_kernel(const MixK m, const ChunkBuf buf, int i0, int i1, int first, int last,
+                        int *keys, int key_bits) {
+  constexpr int K = 2 * DIM;
+  __shared__ float smem_slots[K * DIM * kBlock];
+  __shared__ float smem_acc[K * DIM * kBlock];  // RK4 accumulators of the offsets
+  __shared__ WarpQueue<DIM> smem_queue[kBlock / 32];
+  float *acc = smem_acc + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  WarpQueue<DIM> &wq = smem_queue[threadIdx.x >> 5];
+  const long long N = m.w.N;
+  const long long j_raw = (long long)blockIdx.x * kBlock + threadIdx.x;
+  // lanes past the end mirror the last slot (warp-wide shuffles need every lane) but write nothing
+  const bool active = j_raw < N;
+  const long long j = active ? j_raw : N - 1;
+  const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
+  constexpr bool AB2 = INTEG == FTLE_AB2;
+
+  GroupState<DIM> st;
+  long long g;
+  if (first) {
+    g = j;
+    group_from_positions<DIM>(m, g, st);
+  } else {
+    g = buf.idx[j];
+    state_load<DIM>(buf, N, j, st, AB2);
+  }
+  group_advect<DIM, MODE, INTEG, STORAGE>(m, hd, st, i0, i1, smem_slots, acc, wq, lane);
+  if (!active) return;
+  if (last) {
+    group_finish<DIM>(m, g, st);
+  } else {
+    state_store<DIM>(buf, N, j, st, AB2);
+    buf.idx[j] = g;
+    if (keys) keys[j] = cell_key<DIM>(m, st, key_bits);
+  }
+}
+
 template <int DIM, int MODE, int STORAGE>
-static void launch_mixed(const MixK &m, int integ, cudaStream_t st) {
+static void launch_mixed(const MixK &m, int integ, const ChunkBuf &buf, int i0, int i1,
+                         int first, int last, int *keys, int key_bits, cudaStream_t st) {
   const unsigned blocks = (unsigned)((m.w.N + kBlock - 1) / kBlock);
+#define LM(I)                                                                             \
+  window_mixed_kernel<DIM, MODE, I, STORAGE><<<blocks, kBlock, 0, st>>>(m, buf, i0, i1, first, \
+                                                                         last, keys, key_bits)
   if (integ == FTLE_EULER)
-    window_mixed_kernel<DIM, MODE, FTLE_EULER, STORAGE><<<blocks, kBlock, 0, st>>>(m);
+    LM(FTLE_EULER);
   else if (integ == FTLE_AB2)
-    window_mixed_kernel<DIM, MODE, FTLE_AB2, STORAGE><<<blocks, kBlock, 0, st>>>(m);
+    LM(FTLE_AB2);
   else
-    window_mixed_kernel<DIM, MODE, FTLE_RK4, STORAGE><<<blocks, kBlock, 0, st>>>(m);
+    LM(FTLE_RK4);
+#undef LM
 }
 
-template <int DIM, int MODE>
-static void launch_mixed_s(const MixK &m, int integ, int storage, cudaStream_t st) {
-  if (storage == FTLE_F16)
-    launch_mixed<DIM, MODE, FTLE_F16>(m, integ, st);
-  else if (storage == FTLE_BF16)
-    launch_mixed<DIM, MODE, FTLE_BF16>(m, integ, st);
-  else
-    launch_mixed<DIM, MODE, FTLE_FX15>(m, integ, st);
+static void launch_any(const MixK &m, int dim, int mode, int integ, int storage,
+                       const ChunkBuf &buf, int i0, int i1, int first, int last, int *keys,
+                       int key_bits, cudaStream_t st) {
+#define LS(D, M)                                                                         \
+  do {                                                                                   \
+    if (storage == FTLE_F16)                                                             \
+      launch_mixed<D, M, FTLE_F16>(m, integ, buf, i0, i1, first, last, keys, key_bits, st); \
+    else if (storage == FTLE_BF16)                                                       \
+      launch_mixed<D, M, FTLE_BF16>(m, integ, buf, i0, i1, first, last, keys, key_bits, st); \
+    else                                                                                 \
+      launch_mixed<D, M, FTLE_FX15>(m, integ, buf, i0, i1, first, last, keys, key_bits, st); \
+  } while (0)
+  if (dim == 2) {
+    if (mode == FTLE_HOLD)
+      LS(2, FTLE_HOLD);
+    else
+      LS(2, FTLE_BLEND);
+  } else {
+    if (mode == FTLE_HOLD)
+      LS(3, FTLE_HOLD);
+    else
+      LS(3, FTLE_BLEND);
+  }
+#undef LS
 }
 
-}  // namespace ftle
-
-using namespace ftle;
-
-extern "C" int ftle_window_run_mixed(const ftle_window *w, void *stream) {
-  MixK m;
+static int mixed_setup(const ftle_window *w, MixK &m) {
   int rc = window_to_kernel(w, &m.w);
   if (rc) return rc;
   if (w->storage != FTLE_F16 && w->storage != FTLE_BF16 && w->storage != FTLE_FX15)
-    return fail_invalid("ftle_window_run_mixed needs FTLE_F16, FTLE_BF16 or FTLE_FX15 storage");
-  if (m.w.N == 0) return FTLE_OK;
+    return fail_invalid("the mixed-precision window needs FTLE_F16, FTLE_BF16 or FTLE_FX15 storage");
   if (m.w.g.nodes >= (1LL << 31))
     return fail_invalid("the mixed-precision window supports grids below 2^31 nodes");
   for (int a = 0; a < 3; ++a) {
@@ -827,17 +1039,128 @@ extern "C" int ftle_window_run_mixed(const ftle_window *w, void *stream) {
   }
   m.inv_dt = 1.0 / (w->snapshot_dt != 0.0 ? w->snapshot_dt : 1.0);
   m.inv_S = 1.0 / (double)m.w.num_snaps;
-  cudaStream_t st = as_stream(stream);
-  if (w->grid.dim == 2) {
-    if (w->time_mode == FTLE_HOLD)
-      launch_mixed_s<2, FTLE_HOLD>(m, w->integrator, w->storage, st);
-    else
-      launch_mixed_s<2, FTLE_BLEND>(m, w->integrator, w->storage, st);
+  return FTLE_OK;
+}
+
+// Workspace carve-up: two state buffers, keys, bins.
+struct WsLayout {
+  int64_t state_bytes, keys_off, bins_off, total;
+  int key_bits, nbins;
+};
+
+static int64_t align256(int64_t x) { return (x + 255) & ~int64_t(255); }
+
+static WsLayout ws_layout(int dim, int integ, int64_t N) {
+  const int K = 2 * dim;
+  WsLayout L;
+  int64_t per = 0;
+  per += align256(8 * dim * N);                 // c
+  per += align256(4 * dim * N);                 // wraps
+  per += align256(4 * K * dim * N);             // d
+  per += align256(8 * dim * N);                 // id
+  per += integ == FTLE_AB2 ? align256(4 * (dim + K * dim) * N) : 0;  // AB2 history
+  per += align256(8 * N);                       // idx
+  L.state_bytes = per;
+  L.keys_off = 2 * per;
+  L.bins_off = L.keys_off + align256(4 * N);
+  L.key_bits = dim == 2 ? 8 : 5;
+  L.nbins = 1 << (L.key_bits * dim);
+  L.total = L.bins_off + align256(4 * (int64_t)L.nbins);
+  return L;
+}
+
+static ChunkBuf carve(unsigned char *base, int dim, int integ, int64_t N) {
+  const int K = 2 * dim;
+  ChunkBuf b;
+  unsigned char *p = base;
+  b.c = reinterpret_cast<double *>(p);
+  p += align256(8 * dim * N);
+  b.wraps = reinterpret_cast<int *>(p);
+  p += align256(4 * dim * N);
+  b.d = reinterpret_cast<float *>(p);
+  p += align256(4 * K * dim * N);
+  b.id = reinterpret_cast<double *>(p);
+  p += align256(8 * dim * N);
+  if (integ == FTLE_AB2) {
+    b.hist = reinterpret_cast<float *>(p);
+    p += align256(4 * (dim + K * dim) * N);
   } else {
-    if (w->time_mode == FTLE_HOLD)
-      launch_mixed_s<3, FTLE_HOLD>(m, w->integrator, w->storage, st);
-    else
-      launch_mixed_s<3, FTLE_BLEND>(m, w->integrator, w->storage, st);
+    b.hist = nullptr;
   }
+  b.idx = reinterpret_cast<long long *>(p);
+  return b;
+}
+
+}  // namespace ftle
+
+using namespace ftle;
+
+extern "C" {
+
+int ftle_window_run_mixed(const ftle_window *w, void *stream) {
+  MixK m;
+  int rc = mixed_setup(w, m);
+  if (rc) return rc;
+  if (m.w.N == 0) return FTLE_OK;
+  ChunkBuf none{};
+  launch_any(m, w->grid.dim, w->time_mode, w->integrator, w->storage, none, 0, w->num_steps, 1, 1,
+             nullptr, 0, as_stream(stream));
   return check_launch("window_mixed_kernel");
 }
+
+int64_t ftle_window_workspace_bytes(const ftle_window *w) {
+  if (!w || (w->grid.dim != 2 && w->grid.dim != 3) || w->num_groups < 0) return -1;
+  return ws_layout(w->grid.dim, w->integrator, w->num_groups).total;
+}
+
+int ftle_window_run_mixed_chunked(const ftle_window *w, void *workspace, int64_t workspace_bytes,
+                                  int32_t chunk_steps, int32_t sort_every, void *stream) {
+  MixK m;
+  int rc = mixed_setup(w, m);
+  if (rc) return rc;
+  if (m.w.N == 0) return FTLE_OK;
+  if (chunk_steps < 1) return fail_invalid("chunk_steps must be >= 1");
+  const int dim = w->grid.dim;
+  const WsLayout L = ws_layout(dim, w->integrator, m.w.N);
+  if (!workspace || workspace_bytes < L.total)
+    return fail_invalid("workspace too small: need %lld bytes", (long long)L.total);
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail_invalid("workspace must be 256-byte aligned");
+  cudaStream_t st = as_stream(stream);
+  unsigned char *ws = static_cast<unsigned char *>(workspace);
+  ChunkBuf cur = carve(ws, dim, w->integrator, m.w.N);
+  ChunkBuf nxt = carve(ws + L.state_bytes, dim, w->integrator, m.w.N);
+  int *keys = reinterpret_cast<int *>(ws + L.keys_off);
+  int *bins = reinterpret_cast<int *>(ws + L.bins_off);
+  const int steps = w->num_steps;
+  int chunk = 0;
+  for (int i0 = 0;; i0 += chunk_steps, ++chunk) {
+    const int i1 = i0 + chunk_steps < steps ? i0 + chunk_steps : steps;
+    const int first = i0 == 0, last = i1 == steps;
+    const bool sort_now = !last && sort_every > 0 && (chunk + 1) % sort_every == 0;
+    launch_any(m, dim, w->time_mode, w->integrator, w->storage, cur, i0, i1, first, last,
+               sort_now ? keys : nullptr, L.key_bits, st);
+    if ((rc = check_launch("window_mixed_kernel"))) return rc;
+    if (last) break;
+    if (sort_now) {
+      if (cudaMemsetAsync(bins, 0, 4 * (size_t)L.nbins, st) != cudaSuccess)
+        return check_launch("cudaMemsetAsync");
+      const unsigned b = grid_blocks(m.w.N, 256);
+      sort_hist_kernel<<<b, 256, 0, st>>>(keys, m.w.N, bins);
+      sort_scan_kernel<<<1, 1024, 0, st>>>(bins, L.nbins);
+      if (dim == 2)
+        sort_scatter_kernel<2><<<b, 256, 0, st>>>(keys, m.w.N, bins, cur, nxt,
+                                                  w->integrator == FTLE_AB2);
+      else
+        sort_scatter_kernel<3><<<b, 256, 0, st>>>(keys, m.w.N, bins, cur, nxt,
+                                                  w->integrator == FTLE_AB2);
+      if ((rc = check_launch("sort kernels"))) return rc;
+      const ChunkBuf t = cur;
+      cur = nxt;
+      nxt = t;
+    }
+  }
+  return FTLE_OK;
+}
+
+}  // extern "C"

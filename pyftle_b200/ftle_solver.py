@@ -63,7 +63,9 @@ class FTLESolver:
                               integrator=self.integrator.name, time_mode=spec.time_mode,
                               h=spec.h, num_steps=spec.num_steps, map_period=spec.map_period,
                               t0=spec.t0, first_snapshot=spec.first_snapshot,
-                              snapshot_t0=spec.snapshot_t0, snapshot_dt=spec.snapshot_dt)
+                              snapshot_t0=spec.snapshot_t0, snapshot_dt=spec.snapshot_dt,
+                              chunk_steps=self.options.chunk_steps,
+                              sort_every=self.options.sort_every)
             if self.progress_queue:
                 for i in range(spec.num_steps):
                     self.progress_queue.put((ident, i))

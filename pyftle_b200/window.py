@@ -35,6 +35,8 @@ class EngineOptions:
     precision: str = "fp64"      # "fp64" (plain, reference arithmetic) | "fx15" | "fp16" | "bf16"
     time_mode: str = "hold"      # "hold" (reference) | "blend"
     periodic_time: bool = False  # snapshot index wraps modulo the series length
+    chunk_steps: Optional[int] = None  # mixed path: steps per launch (None: one launch)
+    sort_every: int = 1          # mixed chunked path: cell-sort the groups every n chunks
 
 
 class SnapshotSeries:
@@ -104,8 +106,16 @@ def run_window(series: SnapshotSeries, positions: torch.Tensor, *, integrator: s
                map_period: Optional[float] = None, t0: float = 0.0, first_snapshot: int = 0,
                snapshot_t0: float = 0.0, snapshot_dt: Optional[float] = None,
                ftle_out: Optional[torch.Tensor] = None, with_ftle: bool = True,
-               stream: Optional[torch.cuda.Stream] = None) -> Optional[torch.Tensor]:
-    """Advect ``positions`` (in place) through one window; return the FTLE field."""
+               stream: Optional[torch.cuda.Stream] = None, chunk_steps: Optional[int] = None,
+               sort_every: int = 1,
+               workspace: Optional[torch.Tensor] = None) -> Optional[torch.Tensor]:
+    """Advect ``positions`` (in place) through one window; return the FTLE field.
+
+    Mixed precision only: ``chunk_steps`` splits the window into launches of that
+    many steps with the group state in a device workspace (allocated here unless
+    ``workspace`` is given) and a cell sort of the groups every ``sort_every``
+    chunks.
+    """
     if time_mode not in _lib.TIME_MODES:
         raise ValueError(f"time_mode must be one of {list(_lib.TIME_MODES)}")
     if integrator.lower() not in _lib.INTEGRATOR_CODES:
@@ -124,6 +134,14 @@ def run_window(series: SnapshotSeries, positions: torch.Tensor, *, integrator: s
                           h=h, num_steps=num_steps, map_period=map_period, t0=t0,
                           first_snapshot=first_snapshot, snapshot_t0=snapshot_t0,
                           snapshot_dt=snapshot_dt)
-    fn = "ftle_window_run_f64" if series.storage == _lib.F64 else "ftle_window_run_mixed"
-    _lib.call(fn, w, stream_ptr(stream))
+    if series.storage == _lib.F64:
+        _lib.call("ftle_window_run_f64", w, stream_ptr(stream))
+    elif chunk_steps is None or n == 0:
+        _lib.call("ftle_window_run_mixed", w, stream_ptr(stream))
+    else:
+        need = _lib.load().ftle_window_workspace_bytes(w)
+        if workspace is None or workspace.numel() < need:
+            workspace = torch.empty(max(need, 256), dtype=torch.uint8, device=positions.device)
+        _lib.call("ftle_window_run_mixed_chunked", w, workspace.data_ptr(), workspace.numel(),
+                  int(chunk_steps), int(sort_every), stream_ptr(stream))
     return ftle

@@ -374,3 +374,38 @@ def test_mixed_3d_abc_error(integrator, precision, tol):
     err = rel_l2(ftle, f_ref)
     print(f"{precision} 3D {integrator} FTLE rel L2 error vs FP64 oracle: {err:.3e}")
     assert err < tol
+
+
+@pytest.mark.parametrize("integrator", ["euler", "ab2", "rk4"])
+@pytest.mark.parametrize("chunk,sort_every", [(7, 1), (25, 2), (1000, 1)])
+def test_mixed_chunked_sorted_equals_single_launch(integrator, chunk, sort_every):
+    """Chunking and cell-sorting the groups leave every group's arithmetic unchanged."""
+    n = 32
+    ax = flows.periodic_axis(n)
+    S = 8
+    snaps = flows.abc_snapshots(ax, ax, ax, np.arange(S) * (2 * math.pi / S))
+    pts = flows.grid_points_3d(ax, ax, ax)
+    grid = GridSpec.from_points(pts, (n, n, n), periodic=True)
+    series = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+    cents = np.random.default_rng(11).uniform(0, 2 * math.pi, (1000, 3))
+    pos = flows.seeds_3d(cents, 1e-3)
+    kw = dict(integrator=integrator, time_mode="blend", h=0.02, num_steps=60,
+              snapshot_dt=2 * math.pi / S)
+    p1 = torch.as_tensor(pos, device="cuda")
+    f1 = run_window(series, p1, **kw)
+    p2 = torch.as_tensor(pos, device="cuda")
+    f2 = run_window(series, p2, chunk_steps=chunk, sort_every=sort_every, **kw)
+    np.testing.assert_array_equal(host(p2), host(p1))
+    np.testing.assert_array_equal(host(f2), host(f1))
+
+
+def test_mixed_chunked_2d_nonperiodic_equals_single_launch():
+    shape, pts, snaps, pos = _blend_case_2d(50, 25)
+    series = SnapshotSeries(GridSpec.from_points(pts, shape), snaps, precision="fx15")
+    kw = dict(integrator="rk4", time_mode="blend", h=0.013, num_steps=40, snapshot_dt=0.05)
+    p1 = torch.as_tensor(pos, device="cuda")
+    f1 = run_window(series, p1, **kw)
+    p2 = torch.as_tensor(pos, device="cuda")
+    f2 = run_window(series, p2, chunk_steps=9, sort_every=1, **kw)
+    np.testing.assert_array_equal(host(p2), host(p1))
+    np.testing.assert_array_equal(host(f2), host(f1))
