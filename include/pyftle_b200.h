@@ -182,6 +182,19 @@ int ftle_window_run_mixed_chunked(const ftle_window *w, void *workspace,
                                   int64_t workspace_bytes, int32_t chunk_steps,
                                   int32_t sort_every, void *stream);
 
+/* ftle_window_run_mixed_chunked for callers that cannot provide or allocate
+ * device memory (a host program owning all device memory through its own
+ * pool, a plugin barred from calling cudaMalloc): the workspace is a 32 MiB
+ * array built into the library, reserved on every GPU that loads it until
+ * the process exits.  No counterpart in the reference.  Windows needing more
+ * than 32 MiB (ftle_window_workspace_bytes) are rejected with
+ * FTLE_ERR_INVALID.  The first call on a device looks up the array's device
+ * address, so make it before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other threads) race
+ * and must be serialised by the caller. */
+int ftle_window_run_mixed_chunked_static(const ftle_window *w, int32_t chunk_steps,
+                                         int32_t sort_every, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

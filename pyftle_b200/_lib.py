@@ -72,6 +72,8 @@ SIGNATURES = {
     "ftle_window_workspace_bytes": (ctypes.c_int64, [ctypes.POINTER(FtleWindow)]),
     "ftle_window_run_mixed_chunked": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp, _i64,
                                                      _i32, _i32, _c_dp]),
+    "ftle_window_run_mixed_chunked_static": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32,
+                                                            _i32, _c_dp]),
 }
 
 _lock = threading.Lock()

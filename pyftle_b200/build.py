@@ -30,6 +30,7 @@ SOURCES = {
     "api.cu": [],
     "plain_f64.cu": ["-fmad=false"],
     "mixed.cu": [],
+    "no_alloc.cu": [],
 }
 HEADERS = ["common.cuh"]
 
