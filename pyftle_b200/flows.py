@@ -158,8 +158,11 @@ class FourierTurbulence2D:
     """Divergence-free 2D random-mode field on the periodic box [0, L)^2.
 
     psi(x, t) = sum_m a_m cos(k_m . x + phi_m + w_m t); u = dpsi/dy, v = -dpsi/dx.
-    Mode amplitudes follow E(k) ~ k^(-5/3) for integer wavenumbers
-    kmin <= |k| <= kmax; the field is normalised to unit rms speed.
+    Wavenumbers are integer pairs with kmin <= |k| <= kmax (drawn log-uniformly in |k|,
+    uniformly in angle); amplitudes follow E(k) ~ k^(-5/3); seeded phases and
+    frequencies.  The field is normalised to unit rms speed.  Snapshots on an n x n
+    grid (n > 2*kmax) are exact sums of the modes, evaluated by one inverse FFT of the
+    sparse spectrum per component.
     """
 
     def __init__(self, seed: int = 0, num_modes: int = 256, kmin: float = 4.0,
@@ -168,36 +171,49 @@ class FourierTurbulence2D:
         self.length = length
         kk = np.exp(rng.uniform(math.log(kmin), math.log(kmax), num_modes))
         theta = rng.uniform(0.0, 2.0 * math.pi, num_modes)
-        k0 = 2.0 * math.pi / length
-        kx = np.round(kk * np.cos(theta))
-        ky = np.round(kk * np.sin(theta))
+        kx = np.round(kk * np.cos(theta)).astype(np.int64)
+        ky = np.round(kk * np.sin(theta)).astype(np.int64)
         bad = (kx == 0) & (ky == 0)
-        kx[bad] = kmin
+        kx[bad] = int(kmin)
+        self.ikx, self.iky = kx, ky
         kmag = np.hypot(kx, ky)
-        # log-uniform sampling has density ~1/k, so E(k) ~ k^-5/3 needs
-        # amplitude^2 ~ k^-5/3 * k / k^2 (2D shell) -> psi amplitude ~ k^(-11/6) * k^(1/2)
-        amp = kmag ** (-5.0 / 6.0) / kmag
+        # log-uniform |k| has density ~1/k; E(k) ~ k^-5/3 then needs |u_k|^2 ~ k^-5/3 * k,
+        # i.e. psi amplitude ~ k^(-1/3) / k
+        amp = kmag ** (-1.0 / 3.0) / kmag
+        k0 = 2.0 * math.pi / length
         self.kx = kx * k0
         self.ky = ky * k0
         self.phase = rng.uniform(0.0, 2.0 * math.pi, num_modes)
         self.omega = omega_scale * rng.standard_normal(num_modes)
-        # normalise rms speed to 1
         speed2 = 0.5 * np.sum((amp * self.kx) ** 2 + (amp * self.ky) ** 2)
         self.amp = amp / math.sqrt(speed2)
 
+    def velocity(self, t: float, pts: np.ndarray) -> np.ndarray:
+        """Closed-form velocity at (M, 2) points (direct mode sum; for checks)."""
+        th = np.outer(pts[:, 0], self.kx) + np.outer(pts[:, 1], self.ky) + (
+            self.phase + self.omega * t)
+        s = np.sin(th)
+        out = np.empty((pts.shape[0], 2))
+        out[:, 0] = s @ (self.amp * -self.ky)
+        out[:, 1] = s @ (self.amp * self.kx)
+        return out
+
     def snapshot(self, n: int, t: float) -> np.ndarray:
-        """(2, n*n) velocity on the n x n periodic grid (j*n + i flattening)."""
-        x = periodic_axis(n, self.length)
-        u = np.zeros((n, n))
-        v = np.zeros((n, n))
-        for m in range(len(self.amp)):
-            ph = self.phase[m] + self.omega[m] * t
-            cx = np.exp(1j * (self.kx[m] * x))  # along i (x)
-            cy = np.exp(1j * (self.ky[m] * x + ph))  # along j (y)
-            s = -np.imag(np.outer(cy, cx))  # sin(kx x + ky y + ph) at [j, i]
-            u += self.amp[m] * (-self.ky[m]) * s
-            v += self.amp[m] * (self.kx[m]) * s
-        return np.stack((u.ravel(), v.ravel()))
+        """(2, n*n) velocity on the n x n periodic grid (node (i, j) at j*n + i)."""
+        if n <= 2 * int(np.max(np.abs(np.concatenate([self.ikx, self.iky])))):
+            raise ValueError("grid too coarse for the mode set")
+        ph = self.phase + self.omega * t
+        out = np.empty((2, n * n))
+        for comp, coef in ((0, self.amp * -self.ky), (1, self.amp * self.kx)):
+            # component = sum_m coef_m sin(kx x + ky y + ph_m); with spectrum S[ky, kx],
+            # f(x) = sum S e^{i k.x} and sin th = (e^{i th} - e^{-i th}) / (2i)
+            spec = np.zeros((n, n), dtype=np.complex128)
+            c = coef * np.exp(1j * ph) / 2j
+            np.add.at(spec, (self.iky % n, self.ikx % n), c)
+            np.add.at(spec, ((-self.iky) % n, (-self.ikx) % n), np.conj(c))
+            f = np.fft.ifft2(spec) * (n * n)  # rows: y (j), columns: x (i)
+            out[comp] = f.real.ravel()
+        return out
 
     def snapshots(self, n: int, times) -> np.ndarray:
         return np.stack([self.snapshot(n, float(t)) for t in times])
