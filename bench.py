@@ -49,12 +49,17 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["abc", "batched"], default="abc",
+                   help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
+                        "turbulence windows in one persistent launch")
     p.add_argument("--precision", choices=["fx15", "fp16", "bf16", "fp64"], default="fx15")
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--snapshots", type=int, default=64)
     p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
     p.add_argument("--h", type=float, default=0.02)
     p.add_argument("--T", type=float, default=8.0)
+    p.add_argument("--urms", type=float, default=0.02,
+                   help="batched workload: rms speed of the turbulence field")
     p.add_argument("--chunk-steps", type=int, default=50,
                    help="mixed path: steps per launch between cell sorts (0: one launch)")
     p.add_argument("--sort-every", type=int, default=1)
@@ -451,10 +456,115 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """64 uneven FTLE windows over 2D random-Fourier turbulence in one persistent launch.
+
+    1024^2 periodic grid over [0, 2pi)^2, 400 FX15 snapshots at dt = 0.05; window i:
+    seed grid nx x nx/2 with nx log-uniform in [64, 1024], length U[2, 20], start
+    uniform in [0, 20 - length], RK4 h = 0.025, 4 neighbours at delta = 5e-4.
+    """
+    import torch
+
+    from pyftle_b200 import SnapshotSeries, flows, run_window
+    from pyftle_b200.batch import WindowBatch, WindowSpecRun
+    from pyftle_b200.interpolate import GridSpec
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rng = np.random.default_rng(2026)
+    n, S, dt, h = 1024, 400, 0.05, 0.025
+    L = 2 * math.pi
+    turb = flows.FourierTurbulence2D(seed=7, num_modes=256, kmin=4, kmax=128, urms=args.urms)
+    t_gen = time.time()
+    snaps = turb.snapshots_device(n, np.arange(S) * dt)
+    ax = flows.periodic_axis(n)
+    grid = GridSpec(shape=(n, n), origin=(0.0, 0.0), spacing=(ax[1], ax[1]), periodic=True)
+    series = SnapshotSeries(grid, snaps, precision=args.precision if args.precision != "fp64"
+                            else "fx15")
+    torch.cuda.synchronize()
+    t_gen = time.time() - t_gen
+    wins, pristine = [], []
+    for i in range(64):
+        nx = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
+        ny = max(1, nx // 2)
+        length = rng.uniform(2.0, 20.0)
+        steps = int(round(length / h))
+        t0 = rng.uniform(0.0, (S - 1) * dt - steps * h)
+        cx = (np.arange(nx) + 0.5) * (L / nx)
+        cy = (np.arange(ny) + 0.5) * (L / ny)
+        X, Y = np.meshgrid(cx, cy)
+        pos = torch.from_numpy(flows.seeds_2d(np.column_stack((X.ravel(), Y.ravel())), 5e-4)).cuda()
+        pristine.append(pos.clone())
+        wins.append(WindowSpecRun(pos, t0, h, steps))
+    batch = WindowBatch(series, wins, snapshot_dt=dt)
+
+    def reset():
+        for w, p in zip(wins, pristine):
+            w.positions.copy_(p)
+
+    best = batch.autotune(prologue=reset, use_cache=False)
+    batch.capture(prologue=reset)
+    for _ in range(args.warmup):
+        batch.replay()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        batch.replay()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    ps = batch.particle_steps
+    value = ps / (ms / 1e3)
+    # plain FP64, one launch per window, on every 8th window (same windows' FTLE compared)
+    series64 = SnapshotSeries(grid, snaps, precision="fp64")
+    sel = list(range(0, 64, 8))
+    ps64, ms64, errs, ftle_stats = 0, 0.0, [], []
+    for i in sel:
+        w = wins[i]
+        p = pristine[i].clone()
+        run_window(series64, p, integrator="rk4", time_mode="blend", h=h, num_steps=w.num_steps,
+                   t0=w.t0, snapshot_dt=dt)  # warm-up
+        p.copy_(pristine[i])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f64 = run_window(series64, p, integrator="rk4", time_mode="blend", h=h,
+                         num_steps=w.num_steps, t0=w.t0, snapshot_dt=dt)
+        e1.record()
+        torch.cuda.synchronize()
+        ms64 += e0.elapsed_time(e1)
+        ps64 += pristine[i].shape[0] * w.num_steps
+        errs.append(float(torch.linalg.vector_norm(w.ftle - f64) / torch.linalg.vector_norm(f64)))
+        ftle_stats.append((float(f64.mean()), float(f64.max()), w.num_steps * h))
+    plain = ps64 / (ms64 / 1e3)
+    line = {
+        "metric": METRIC + " (batched windows)", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "64 uneven 2D turbulence windows, 1024^2 periodic grid, 400 "
+                               "snapshots, seed grids 64x32..1024x512, lengths U[2,20], RK4 "
+                               "h=0.025, one persistent CUDA-graph launch",
+                   "precision": series.precision, "windows": 64, "urms": args.urms,
+                   "particles": sum(w.positions.shape[0] for w in wins),
+                   "particle_steps": ps, "schedule": {"ctas_per_sm": best.ctas_per_sm,
+                                                      "order": best.order},
+                   "autotune_ms": batch.tuning, "snapshot_build_s": t_gen},
+        "ftle_fields_per_s": 64 / (ms / 1e3),
+        "plain_fp64": {"value": plain, "windows": len(sel),
+                       "speedup_chosen_vs_plain": value / plain,
+                       "ftle_rel_err_l2_per_window": errs,
+                       "ftle_mean_max_T_per_window": ftle_stats},
+        "gpu_launches": args.steps * 1,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

@@ -182,6 +182,23 @@ int ftle_window_run_mixed_chunked(const ftle_window *w, void *workspace,
                                   int64_t workspace_bytes, int32_t chunk_steps,
                                   int32_t sort_every, void *stream);
 
+/* ---- many windows in one persistent launch -------------------------------
+ * Windows that share one packed snapshot series, grid, storage, time mode and
+ * integrator, but differ in seed set, start time t0, step h, length and
+ * map_period, run as one launch: persistent CTAs take work items (128 groups of
+ * one window) from a counter until all are done.  Replaces the reference's
+ * one-process-per-window ParallelExecutor (parallel.py:171-271) for the hot
+ * path.  Build the plan once on the host (ftle_windows_plan: window table plus
+ * work list; order 1 = longest windows first, 0 = as given), copy it to a
+ * 256-byte aligned device buffer, then run it any number of times; the plan
+ * holds the windows' device pointers.  The run only issues a memset of the
+ * plan's counter and one kernel on `stream`. */
+int64_t ftle_windows_plan_bytes(const ftle_window *windows, int32_t count);
+int ftle_windows_plan(const ftle_window *windows, int32_t count, int32_t order,
+                      void *host_plan, int64_t plan_bytes);
+int ftle_windows_run_mixed(const ftle_window *windows, int32_t count, void *device_plan,
+                           int64_t plan_bytes, int32_t ctas_per_sm, void *stream);
+
 /* ftle_window_run_mixed_chunked for callers that cannot provide or allocate
  * device memory (a host program owning all device memory through its own
  * pool, a plugin barred from calling cudaMalloc): the workspace is a 32 MiB

@@ -74,6 +74,10 @@ SIGNATURES = {
                                                      _i32, _i32, _c_dp]),
     "ftle_window_run_mixed_chunked_static": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32,
                                                             _i32, _c_dp]),
+    "ftle_windows_plan_bytes": (ctypes.c_int64, [ctypes.POINTER(FtleWindow), _i32]),
+    "ftle_windows_plan": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32, _i32, _c_dp, _i64]),
+    "ftle_windows_run_mixed": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32, _c_dp, _i64,
+                                              _i32, _c_dp]),
 }
 
 _lock = threading.Lock()

@@ -246,6 +246,28 @@ struct MixK {
   double inv_S;       // 1/num_snapshots
 };
 
+// Per-window values (one window: taken from MixK; a batch: one entry per window).
+struct WinVar {
+  double t0, h, map_period;
+  double *positions;
+  double *ftle;
+  long long N;
+  int num_steps, first_snapshot;
+};
+
+__device__ __forceinline__ WinVar winvar_of(const MixK &m) {
+  WinVar v;
+  v.t0 = m.w.t0;
+  v.h = m.w.h;
+  v.map_period = m.w.map_period;
+  v.positions = m.w.positions;
+  v.ftle = m.w.ftle;
+  v.N = m.w.N;
+  v.num_steps = m.w.num_steps;
+  v.first_snapshot = m.w.first_snapshot;
+  return v;
+}
+
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
 
 // Wrap a cell index into [0, n): one conditional step covers every index
@@ -381,13 +403,13 @@ __device__ __forceinline__ float poly_diff(const float *A, const float *f, const
 }
 
 template <int DIM, int MODE>
-__device__ __forceinline__ const unsigned char *record_set(const MixK &m, int step, double t,
-                                                           float &alpha) {
+__device__ __forceinline__ const unsigned char *record_set(const MixK &m, int first_snapshot,
+                                                           int step, double t, float &alpha) {
   const long long rec_bytes = DIM == 2 ? 8 : 16;
   const unsigned char *base = static_cast<const unsigned char *>(m.w.snaps) + kHeaderBytes;
   int s;
   if constexpr (MODE == FTLE_HOLD) {
-    s = m.w.first_snapshot + step;
+    s = first_snapshot + step;
     if (m.w.periodic_time) s %= m.w.num_snaps;
     alpha = 0.0f;
   } else {
@@ -611,15 +633,15 @@ struct GroupState {
 
 // Centroid = mean of the K neighbours (particles.py:235-236); offsets relative to it.
 template <int DIM>
-__device__ __forceinline__ void group_from_positions(const MixK &m, long long g,
+__device__ __forceinline__ void group_from_positions(const MixK &m, const WinVar &v, long long g,
                                                      GroupState<DIM> &st) {
   constexpr int K = 2 * DIM;
-  const long long N = m.w.N;
+  const long long N = v.N;
   double X[K][DIM];
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) X[k][a] = m.w.positions[((long long)k * N + g) * DIM + a];
+    for (int a = 0; a < DIM; ++a) X[k][a] = v.positions[((long long)k * N + g) * DIM + a];
 #pragma unroll
   for (int a = 0; a < DIM; ++a) {
     double s = X[0][a];
@@ -652,14 +674,14 @@ __device__ __forceinline__ void group_from_positions(const MixK &m, long long g,
 
 // Advect one group through steps [i0, i1) of the window.
 template <int DIM, int MODE, int INTEG, int STORAGE>
-__device__ __forceinline__ void group_advect(const MixK &m, const Header16 &hd,
+__device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, const Header16 &hd,
                                              GroupState<DIM> &st, int i0, int i1,
                                              float *smem_slots, float *acc, WarpQueue<DIM> &wq,
                                              int lane) {
   constexpr int K = 2 * DIM;
   constexpr bool BLEND = MODE == FTLE_BLEND;
   const bool periodic = m.w.g.periodic != 0;
-  const double h = m.w.h;
+  const double h = v.h;
   const float hf = (float)h;
   float kc[DIM], kd[K][DIM], accc[DIM];
 #pragma unroll
@@ -671,7 +693,7 @@ __device__ __forceinline__ void group_advect(const MixK &m, const Header16 &hd,
 
   constexpr int NST = INTEG == FTLE_RK4 ? 4 : 1;
   for (int i = i0; i < i1; ++i) {
-    const double t = m.w.t0 + (double)i * h;
+    const double t = v.t0 + (double)i * h;
 #pragma unroll 1
     for (int s = 0; s < NST; ++s) {
       // RK4 tableau: stage point x + a*k_prev, weight w, time t + tc*h
@@ -679,7 +701,8 @@ __device__ __forceinline__ void group_advect(const MixK &m, const Header16 &hd,
       const float as = tc * hf;
       const float ws = (s == 0 || s == 3) ? 1.0f : 2.0f;
       float alpha;
-      const unsigned char *recs = record_set<DIM, MODE>(m, i, t + (double)tc * h, alpha);
+      const unsigned char *recs =
+          record_set<DIM, MODE>(m, v.first_snapshot, i, t + (double)tc * h, alpha);
       double cs[DIM];
 #pragma unroll
       for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], st.c[a]);
@@ -762,9 +785,10 @@ __device__ __forceinline__ void group_advect(const MixK &m, const Header16 &hd,
 
 // Final positions x_k = c + wraps*period + d_k and the FP64 FTLE epilogue.
 template <int DIM>
-__device__ __forceinline__ void group_finish(const MixK &m, long long g, GroupState<DIM> &st) {
+__device__ __forceinline__ void group_finish(const MixK &m, const WinVar &v, long long g,
+                                             GroupState<DIM> &st) {
   constexpr int K = 2 * DIM;
-  const long long N = m.w.N;
+  const long long N = v.N;
   double c[DIM];
 #pragma unroll
   for (int a = 0; a < DIM; ++a)
@@ -773,8 +797,8 @@ __device__ __forceinline__ void group_finish(const MixK &m, long long g, GroupSt
   for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
-      m.w.positions[((long long)k * N + g) * DIM + a] = c[a] + (double)st.d[k][a];
-  if (m.w.ftle != nullptr) {
+      v.positions[((long long)k * N + g) * DIM + a] = c[a] + (double)st.d[k][a];
+  if (v.ftle != nullptr) {
     double J[DIM][DIM];
 #pragma unroll
     for (int i = 0; i < DIM; ++i)
@@ -793,7 +817,7 @@ __device__ __forceinline__ void group_finish(const MixK &m, long long g, GroupSt
           C[i][k] = J[i][0] * J[k][0] + J[i][1] * J[k][1] + J[i][2] * J[k][2];
       lam = lmax3_sym(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
     }
-    m.w.ftle[g] = (1.0 / m.w.map_period) * log(sqrt(lam));
+    v.ftle[g] = (1.0 / v.map_period) * log(sqrt(lam));
   }
 }
 
@@ -953,24 +977,126 @@ __global__ void __launch_bounds__(kBlock, 3)
   const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
   constexpr bool AB2 = INTEG == FTLE_AB2;
 
+  const WinVar v = winvar_of(m);
   GroupState<DIM> st;
   long long g;
   if (first) {
     g = j;
-    group_from_positions<DIM>(m, g, st);
+    group_from_positions<DIM>(m, v, g, st);
   } else {
     g = buf.idx[j];
     state_load<DIM>(buf, N, j, st, AB2);
   }
-  group_advect<DIM, MODE, INTEG, STORAGE>(m, hd, st, i0, i1, smem_slots, acc, wq, lane);
+  group_advect<DIM, MODE, INTEG, STORAGE>(m, v, hd, st, i0, i1, smem_slots, acc, wq, lane);
   if (!active) return;
   if (last) {
-    group_finish<DIM>(m, g, st);
+    group_finish<DIM>(m, v, g, st);
   } else {
     state_store<DIM>(buf, N, j, st, AB2);
     buf.idx[j] = g;
     if (keys) keys[j] = cell_key<DIM>(m, st, key_bits);
   }
+}
+
+// ---------------------------------------------------------------------------
+// many windows in one persistent launch
+// ---------------------------------------------------------------------------
+
+// A work item: kBlock consecutive groups of one window.
+struct BatchItem {
+  int window;
+  int reserved;
+  long long g0;
+};
+
+// Plan layout (host-built, copied to the device once):
+//   PlanHeader | WinVar[num_windows] | BatchItem[num_items] | int counter
+struct PlanHeader {
+  int num_windows, num_items, order, reserved;
+};
+
+static int64_t align256_(int64_t x) { return (x + 255) & ~int64_t(255); }
+static int64_t plan_offset_wins() { return 256; }
+static int64_t plan_offset_items(int nw) { return align256_(256 + (int64_t)nw * sizeof(WinVar)); }
+static int64_t plan_offset_counter(int nw, int64_t ni) {
+  return align256_(plan_offset_items(nw) + ni * (int64_t)sizeof(BatchItem));
+}
+static int64_t plan_total(int nw, int64_t ni) { return plan_offset_counter(nw, ni) + 256; }
+
+// Persistent CTAs take work items from a global counter until the list is empty;
+// every thread of an item advects one group of that item's window.
+template <int DIM, int MODE, int INTEG, int STORAGE>
+__global__ void __launch_bounds__(kBlock, 3)
+    windows_persistent_kernel(const MixK m, const WinVar *__restrict__ wins,
+                              const BatchItem *__restrict__ items, int num_items, int *counter) {
+  constexpr int K = 2 * DIM;
+  __shared__ float smem_slots[K * DIM * kBlock];
+  __shared__ float smem_acc[K * DIM * kBlock];
+  __shared__ WarpQueue<DIM> smem_queue[kBlock / 32];
+  __shared__ int s_item;
+  float *acc = smem_acc + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  WarpQueue<DIM> &wq = smem_queue[threadIdx.x >> 5];
+  const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();  // every thread has read s_item before thread 0 overwrites it
+    if (it >= num_items) return;
+    const BatchItem bi = items[it];
+    const WinVar v = wins[bi.window];
+    const long long j_raw = bi.g0 + threadIdx.x;
+    const bool active = j_raw < v.N;
+    const long long j = active ? j_raw : v.N - 1;
+    GroupState<DIM> st;
+    group_from_positions<DIM>(m, v, j, st);
+    group_advect<DIM, MODE, INTEG, STORAGE>(m, v, hd, st, 0, v.num_steps, smem_slots, acc, wq,
+                                            lane);
+    if (active) group_finish<DIM>(m, v, j, st);
+  }
+}
+
+template <int DIM, int MODE, int STORAGE>
+static void launch_persistent(const MixK &m, int integ, const WinVar *wins,
+                              const BatchItem *items, int num_items, int *counter, int ctas,
+                              cudaStream_t st) {
+#define LP(I)                                                                        \
+  windows_persistent_kernel<DIM, MODE, I, STORAGE><<<ctas, kBlock, 0, st>>>(m, wins, items, \
+                                                                          num_items, counter)
+  if (integ == FTLE_EULER)
+    LP(FTLE_EULER);
+  else if (integ == FTLE_AB2)
+    LP(FTLE_AB2);
+  else
+    LP(FTLE_RK4);
+#undef LP
+}
+
+static void launch_persistent_any(const MixK &m, int dim, int mode, int integ, int storage,
+                                  const WinVar *wins, const BatchItem *items, int num_items,
+                                  int *counter, int ctas, cudaStream_t st) {
+#define LPS(D, M)                                                                            \
+  do {                                                                                       \
+    if (storage == FTLE_F16)                                                                 \
+      launch_persistent<D, M, FTLE_F16>(m, integ, wins, items, num_items, counter, ctas, st); \
+    else if (storage == FTLE_BF16)                                                           \
+      launch_persistent<D, M, FTLE_BF16>(m, integ, wins, items, num_items, counter, ctas, st); \
+    else                                                                                     \
+      launch_persistent<D, M, FTLE_FX15>(m, integ, wins, items, num_items, counter, ctas, st); \
+  } while (0)
+  if (dim == 2) {
+    if (mode == FTLE_HOLD)
+      LPS(2, FTLE_HOLD);
+    else
+      LPS(2, FTLE_BLEND);
+  } else {
+    if (mode == FTLE_HOLD)
+      LPS(3, FTLE_HOLD);
+    else
+      LPS(3, FTLE_BLEND);
+  }
+#undef LPS
 }
 
 template <int DIM, int MODE, int STORAGE>
@@ -1161,6 +1287,125 @@ int ftle_window_run_mixed_chunked(const ftle_window *w, void *workspace, int64_t
     }
   }
   return FTLE_OK;
+}
+
+// ---- many windows in one launch ------------------------------------------
+
+static int check_batch(const ftle_window *windows, int32_t count) {
+  if (!windows || count < 1) return fail_invalid("need at least one window");
+  const ftle_window &a = windows[0];
+  for (int i = 1; i < count; ++i) {
+    const ftle_window &b = windows[i];
+    if (b.snapshots != a.snapshots || b.num_snapshots != a.num_snapshots ||
+        b.storage != a.storage || b.time_mode != a.time_mode ||
+        b.periodic_time != a.periodic_time || b.snapshot_t0 != a.snapshot_t0 ||
+        b.snapshot_dt != a.snapshot_dt || b.integrator != a.integrator ||
+        b.grid.dim != a.grid.dim || b.grid.periodic != a.grid.periodic)
+      return fail_invalid("window %d does not share window 0's snapshot series and integrator", i);
+    for (int ax = 0; ax < 3; ++ax)
+      if (b.grid.n[ax] != a.grid.n[ax] || b.grid.origin[ax] != a.grid.origin[ax] ||
+          b.grid.spacing[ax] != a.grid.spacing[ax])
+        return fail_invalid("window %d does not share window 0's grid", i);
+  }
+  for (int i = 0; i < count; ++i) {
+    MixK m;
+    int rc = mixed_setup(&windows[i], m);
+    if (rc) return rc;
+  }
+  return FTLE_OK;
+}
+
+static int64_t batch_items(const ftle_window *windows, int32_t count) {
+  int64_t n = 0;
+  for (int i = 0; i < count; ++i) n += (windows[i].num_groups + kBlock - 1) / kBlock;
+  return n;
+}
+
+int64_t ftle_windows_plan_bytes(const ftle_window *windows, int32_t count) {
+  if (!windows || count < 1) return -1;
+  return plan_total(count, batch_items(windows, count));
+}
+
+int ftle_windows_plan(const ftle_window *windows, int32_t count, int32_t order, void *host_plan,
+                      int64_t plan_bytes) {
+  int rc = check_batch(windows, count);
+  if (rc) return rc;
+  const int64_t ni = batch_items(windows, count);
+  if (ni > 0x7fffffff) return fail_invalid("too many work items");
+  if (!host_plan || plan_bytes < plan_total(count, ni))
+    return fail_invalid("plan buffer too small: need %lld bytes", (long long)plan_total(count, ni));
+  unsigned char *p = static_cast<unsigned char *>(host_plan);
+  PlanHeader *hdr = reinterpret_cast<PlanHeader *>(p);
+  hdr->num_windows = count;
+  hdr->num_items = (int)ni;
+  hdr->order = order;
+  hdr->reserved = 0;
+  WinVar *wins = reinterpret_cast<WinVar *>(p + plan_offset_wins());
+  for (int i = 0; i < count; ++i) {
+    const ftle_window &w = windows[i];
+    wins[i].t0 = w.t0;
+    wins[i].h = w.h;
+    wins[i].map_period = w.map_period;
+    wins[i].positions = w.positions;
+    wins[i].ftle = w.ftle;
+    wins[i].N = w.num_groups;
+    wins[i].num_steps = w.num_steps;
+    wins[i].first_snapshot = w.first_snapshot;
+  }
+  // order 1: longest windows first (work items of long windows are scheduled before short
+  // ones so the tail of the persistent launch is short); order 0: as given.
+  int *perm = new int[count];
+  for (int i = 0; i < count; ++i) perm[i] = i;
+  if (order == 1) {
+    for (int i = 1; i < count; ++i) {  // insertion sort by num_steps, descending, stable
+      const int x = perm[i];
+      int k = i - 1;
+      while (k >= 0 && windows[perm[k]].num_steps < windows[x].num_steps) {
+        perm[k + 1] = perm[k];
+        --k;
+      }
+      perm[k + 1] = x;
+    }
+  }
+  BatchItem *items = reinterpret_cast<BatchItem *>(p + plan_offset_items(count));
+  int64_t q = 0;
+  for (int r = 0; r < count; ++r) {
+    const int i = perm[r];
+    for (int64_t g0 = 0; g0 < windows[i].num_groups; g0 += kBlock) {
+      items[q].window = i;
+      items[q].reserved = 0;
+      items[q].g0 = g0;
+      ++q;
+    }
+  }
+  delete[] perm;
+  *reinterpret_cast<int *>(p + plan_offset_counter(count, ni)) = 0;
+  return FTLE_OK;
+}
+
+int ftle_windows_run_mixed(const ftle_window *windows, int32_t count, void *device_plan,
+                           int64_t plan_bytes, int32_t ctas_per_sm, void *stream) {
+  int rc = check_batch(windows, count);
+  if (rc) return rc;
+  const int64_t ni = batch_items(windows, count);
+  if (!device_plan || plan_bytes < plan_total(count, ni))
+    return fail_invalid("plan buffer too small: need %lld bytes", (long long)plan_total(count, ni));
+  if (reinterpret_cast<uintptr_t>(device_plan) % 256 != 0)
+    return fail_invalid("plan must be 256-byte aligned");
+  if (ctas_per_sm < 1 || ctas_per_sm > 3) return fail_invalid("ctas_per_sm must be 1, 2 or 3");
+  if (ni == 0) return FTLE_OK;
+  MixK m;
+  mixed_setup(&windows[0], m);
+  unsigned char *p = static_cast<unsigned char *>(device_plan);
+  int *counter = reinterpret_cast<int *>(p + plan_offset_counter(count, ni));
+  cudaStream_t st = as_stream(stream);
+  if (cudaMemsetAsync(counter, 0, sizeof(int), st) != cudaSuccess)
+    return check_launch("cudaMemsetAsync");
+  launch_persistent_any(m, windows[0].grid.dim, windows[0].time_mode, windows[0].integrator,
+                        windows[0].storage, reinterpret_cast<const WinVar *>(p + plan_offset_wins()),
+                        reinterpret_cast<const BatchItem *>(p + plan_offset_items(count)), (int)ni,
+                        counter, ctas_per_sm * kNumSMs, st);
+  return check_launch("windows_persistent_kernel");
 }
 
 }  // extern "C"

@@ -160,13 +160,14 @@ class FourierTurbulence2D:
     psi(x, t) = sum_m a_m cos(k_m . x + phi_m + w_m t); u = dpsi/dy, v = -dpsi/dx.
     Wavenumbers are integer pairs with kmin <= |k| <= kmax (drawn log-uniformly in |k|,
     uniformly in angle); amplitudes follow E(k) ~ k^(-5/3); seeded phases and
-    frequencies.  The field is normalised to unit rms speed.  Snapshots on an n x n
+    frequencies.  The field is normalised to rms speed ``urms``.  Snapshots on an n x n
     grid (n > 2*kmax) are exact sums of the modes, evaluated by one inverse FFT of the
     sparse spectrum per component.
     """
 
     def __init__(self, seed: int = 0, num_modes: int = 256, kmin: float = 4.0,
-                 kmax: float = 128.0, length: float = 2.0 * math.pi, omega_scale: float = 1.0):
+                 kmax: float = 128.0, length: float = 2.0 * math.pi, omega_scale: float = 1.0,
+                 urms: float = 1.0):
         rng = np.random.default_rng(seed)
         self.length = length
         kk = np.exp(rng.uniform(math.log(kmin), math.log(kmax), num_modes))
@@ -186,7 +187,7 @@ class FourierTurbulence2D:
         self.phase = rng.uniform(0.0, 2.0 * math.pi, num_modes)
         self.omega = omega_scale * rng.standard_normal(num_modes)
         speed2 = 0.5 * np.sum((amp * self.kx) ** 2 + (amp * self.ky) ** 2)
-        self.amp = amp / math.sqrt(speed2)
+        self.amp = urms * amp / math.sqrt(speed2)
 
     def velocity(self, t: float, pts: np.ndarray) -> np.ndarray:
         """Closed-form velocity at (M, 2) points (direct mode sum; for checks)."""
@@ -217,3 +218,30 @@ class FourierTurbulence2D:
 
     def snapshots(self, n: int, times) -> np.ndarray:
         return np.stack([self.snapshot(n, float(t)) for t in times])
+
+    def snapshots_device(self, n: int, times, device="cuda"):
+        """(S, 2, n*n) float64 torch tensor built on the device (same values as
+        ``snapshots``; input generation only)."""
+        import torch
+
+        if n <= 2 * int(np.max(np.abs(np.concatenate([self.ikx, self.iky])))):
+            raise ValueError("grid too coarse for the mode set")
+        iy = torch.as_tensor(self.iky % n, device=device)
+        ix = torch.as_tensor(self.ikx % n, device=device)
+        iyc = torch.as_tensor((-self.iky) % n, device=device)
+        ixc = torch.as_tensor((-self.ikx) % n, device=device)
+        coefs = [torch.as_tensor(self.amp * -self.ky, device=device),
+                 torch.as_tensor(self.amp * self.kx, device=device)]
+        phase = torch.as_tensor(self.phase, device=device)
+        omega = torch.as_tensor(self.omega, device=device)
+        out = torch.empty((len(times), 2, n * n), dtype=torch.float64, device=device)
+        spec = torch.zeros((n, n), dtype=torch.complex128, device=device)
+        for si, t in enumerate(times):
+            ph = phase + omega * float(t)
+            for comp in range(2):
+                c = coefs[comp] * torch.exp(1j * ph) / 2j
+                spec.zero_()
+                spec.index_put_((iy, ix), c, accumulate=True)
+                spec.index_put_((iyc, ixc), torch.conj(c), accumulate=True)
+                out[si, comp] = (torch.fft.ifft2(spec) * (n * n)).real.reshape(-1)
+        return out
