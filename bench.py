@@ -238,25 +238,19 @@ def run_ours(args):
                              run_window)
     from pyftle_b200.interpolate import GridSpec
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
+    from pyftle_b200 import parallel
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    env = parallel.RankInfo.from_env()
+    torch.cuda.set_device(env.local_rank)
+    info = parallel.init("nccl", timeout_s=600)
+    world, rank, local = info.world, info.rank, info.local_rank
 
     def barrier():
         if world > 1:
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return parallel.max_over_ranks(x, device="cuda")
 
     w = workload(args)
     n = w["n"]
