@@ -42,6 +42,7 @@ class WindowSpecRun:
     num_steps: int
     map_period: Optional[float] = None
     ftle: Optional[torch.Tensor] = None
+    first_snapshot: int = 0  # HOLD windows: snapshot used by step 0
 
 
 @dataclass(frozen=True)
@@ -68,7 +69,8 @@ class WindowBatch:
                 w.ftle = torch.empty(n, dtype=torch.float64, device=w.positions.device)
             mp = w.map_period if w.map_period is not None else w.num_steps * abs(w.h)
             arr[i] = window_descriptor(series, w.positions, w.ftle, h=w.h, num_steps=w.num_steps,
-                                       map_period=mp, t0=w.t0, **self.kw)
+                                       map_period=mp, t0=w.t0, first_snapshot=w.first_snapshot,
+                                       **self.kw)
         self.desc = arr
         self.count = len(self.windows)
         self.graph: Optional[torch.cuda.CUDAGraph] = None

@@ -54,8 +54,8 @@ class FTLESolver:
     def run_device(self) -> torch.Tensor:
         self.particles = self.source.get_particles()
         ident = self.source.id
-        if self._fused_ok():
-            spec = self.source.window_spec()
+        spec = self.source.window_spec() if self._fused_ok() else None
+        if spec is not None:
             precision = self.options.precision
             self.series = SnapshotSeries(spec.grid, spec.snapshots, precision=precision,
                                          periodic_time=spec.periodic_time)

@@ -1,0 +1,318 @@
+"""File I/O around the engine: MATLAB readers, a file-fed BatchSource, writers.
+
+Host-side code (not the hot path), mirroring pyFTLE's ``file_readers.py``,
+``data_source.py`` (``FileBatchSource``) and ``file_writers.py``:
+
+* ``read_velocity`` / ``read_coordinate`` -- ``.mat`` keys ``velocity_x/y(/z)`` and
+  ``coordinate_x/y(/z)``, each raveled in C order and stacked to ``(dim, N)``
+  (file_readers.py:35-118);
+* ``read_seed_particles_coordinates`` -- keys ``left, right, top, bottom(, front,
+  back)`` concatenated in that order into ``NeighboringParticles``
+  (file_readers.py:121-182);
+* ``FileBatchSource`` -- the reference's per-step protocol plus ``window_spec()``:
+  all snapshot files of a window are read by a thread pool into pinned host
+  memory and copied to the device on a side stream while later files are still
+  being read, so the fused path receives a device-resident stack;
+* ``MatWriter`` / ``VTKWriter`` / ``create_writer`` -- ``ftle_<id>.mat`` with keys
+  ``ftle, x, y(, z)`` (reshaped to the grid when ``grid_shape`` is given) and VTK
+  XML ``.vts`` (structured) / ``.vtp`` (point cloud), written directly
+  (file_writers.py:68-302; no pyvista needed).
+"""
+
+from __future__ import annotations
+
+import base64
+import os
+import struct
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+from scipy.io import loadmat, savemat
+
+from pyftle_b200.data_source import WindowSpec
+from pyftle_b200.interpolate import GridSpec, Interpolator
+from pyftle_b200.particles import NeighboringParticles
+
+# ----------------------------------------------------------------------------
+# readers
+# ----------------------------------------------------------------------------
+
+
+def _stack(data: dict, prefix: str, path) -> np.ndarray:
+    if f"{prefix}_x" not in data or f"{prefix}_y" not in data:
+        raise ValueError(f"The MATLAB file {path} does not contain the expected keys "
+                         f"'{prefix}_x' and '{prefix}_y'.")
+    comps = [np.asarray(data[f"{prefix}_x"]).ravel(), np.asarray(data[f"{prefix}_y"]).ravel()]
+    if f"{prefix}_z" in data:
+        comps.append(np.asarray(data[f"{prefix}_z"]).ravel())
+    return np.stack(comps).astype(np.float64, copy=False)
+
+
+def read_velocity(file_path) -> np.ndarray:
+    return _stack(loadmat(file_path), "velocity", file_path)
+
+
+def read_coordinate(file_path) -> np.ndarray:
+    return _stack(loadmat(file_path), "coordinate", file_path)
+
+
+def read_seed_positions(file_path) -> np.ndarray:
+    """Role-blocked (K*N, dim) seed positions: left, right, top, bottom(, front, back)."""
+    data = loadmat(file_path)
+    if any(k not in data for k in ("left", "right", "top", "bottom")):
+        raise ValueError("The MATLAB file must contain at least 'left', 'right', 'top' and "
+                         "'bottom' keys. ('front' and 'back' for 3D)")
+    keys = ["left", "right", "top", "bottom"]
+    if "front" in data and "back" in data:
+        keys += ["front", "back"]
+    return np.concatenate([np.asarray(data[k], dtype=np.float64) for k in keys], axis=0)
+
+
+def read_seed_particles_coordinates(file_path) -> NeighboringParticles:
+    return NeighboringParticles(positions=read_seed_positions(file_path))
+
+
+# ----------------------------------------------------------------------------
+# file-fed source
+# ----------------------------------------------------------------------------
+
+
+class FileBatchSource:
+    """One window fed from ``.mat`` files (data_source.py:86-211), HOLD semantics."""
+
+    def __init__(self, snapshot_files: List[str], coordinate_files: List[str],
+                 particle_file: str, snapshot_timestep: float, flow_map_period,
+                 grid_shape: Optional[tuple] = None, periodic_space: bool = False,
+                 workers: int = 8):
+        self.snapshot_files = list(snapshot_files)
+        self.coordinate_files = list(coordinate_files)
+        self.particle_file = particle_file
+        self.snapshot_timestep = float(snapshot_timestep)
+        self.flow_map_period = flow_map_period
+        self._id = Path(self.snapshot_files[0]).stem
+        self.reuse_coordinates = len(set(self.coordinate_files)) == 1
+        self.grid_shape = tuple(grid_shape) if grid_shape is not None else None
+        self.periodic_space = periodic_space
+        self.workers = workers
+
+    @property
+    def id(self) -> str:
+        return self._id
+
+    @property
+    def num_steps(self) -> int:
+        return len(self.snapshot_files)
+
+    @property
+    def timestep(self) -> float:
+        return self.snapshot_timestep
+
+    def get_particles(self) -> NeighboringParticles:
+        return read_seed_particles_coordinates(self.particle_file)
+
+    def get_data_for_step(self, step_index: int):
+        velocities = read_velocity(self.snapshot_files[step_index])
+        coordinates = None
+        if step_index == 0 or not self.reuse_coordinates:
+            coordinates = read_coordinate(self.coordinate_files[step_index])
+        return velocities, coordinates
+
+    def update_interpolator(self, interpolator: Interpolator, step_index: int) -> None:
+        velocities, coordinates = self.get_data_for_step(step_index)
+        interpolator.update(velocities, coordinates)
+
+    def window_spec(self) -> Optional[WindowSpec]:
+        """Device-resident snapshot stack for the fused path (None for moving grids)."""
+        if not self.reuse_coordinates or self.grid_shape is None:
+            return None
+        points = read_coordinate(self.coordinate_files[0])
+        grid = GridSpec.from_points(points, self.grid_shape, self.periodic_space)
+        snaps = load_snapshots(self.snapshot_files, grid.dim, grid.nodes, workers=self.workers)
+        n = self.num_steps
+        dt = self.snapshot_timestep
+        return WindowSpec(grid=grid, snapshots=snaps, time_mode="hold", h=dt, num_steps=n,
+                          map_period=(n - 1) * abs(dt), snapshot_dt=dt)
+
+
+def load_snapshots(files: Sequence[str], dim: int, nodes: int, workers: int = 8,
+                   device=None) -> torch.Tensor:
+    """Read velocity files in parallel into a (S, dim, nodes) float64 device tensor.
+
+    Files are read by a thread pool into pinned host buffers; each is copied to
+    the device on a side stream as soon as it is read, overlapping the copies
+    with the remaining reads.
+    """
+    device = device or torch.device("cuda", torch.cuda.current_device())
+    out = torch.empty((len(files), dim, nodes), dtype=torch.float64, device=device)
+    copy_stream = torch.cuda.Stream(device=device)
+    staging: List[torch.Tensor] = []
+
+    def read(path):
+        v = read_velocity(path)
+        if v.shape != (dim, nodes):
+            raise ValueError(f"{path}: velocity has shape {v.shape}, expected {(dim, nodes)}")
+        pinned = torch.empty((dim, nodes), dtype=torch.float64).pin_memory()
+        pinned.numpy()[...] = v
+        return pinned
+
+    with ThreadPoolExecutor(max_workers=max(1, workers)) as pool:
+        futures = [pool.submit(read, f) for f in files]
+        with torch.cuda.stream(copy_stream):
+            for i, fut in enumerate(futures):
+                buf = fut.result()
+                out[i].copy_(buf, non_blocking=True)
+                staging.append(buf)  # keep pinned buffers alive until the copies finish
+    torch.cuda.current_stream(device).wait_stream(copy_stream)
+    copy_stream.synchronize()
+    return out
+
+
+# ----------------------------------------------------------------------------
+# writers
+# ----------------------------------------------------------------------------
+
+
+class FTLEWriter:
+    def __init__(self, directory_path, grid_shape: Optional[tuple] = None) -> None:
+        self.path = directory_path
+        os.makedirs(self.path, exist_ok=True)
+        self.grid_shape = grid_shape
+        self.dim: Optional[int] = None
+
+    def write(self, filename: str, ftle_field, particles_centroid) -> None:
+        raise NotImplementedError
+
+
+def _host(a) -> np.ndarray:
+    return a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+
+
+class MatWriter(FTLEWriter):
+    """``<filename>.mat`` with keys ftle, x, y(, z) (file_writers.py:68-164)."""
+
+    def write(self, filename: str, ftle_field, particles_centroid) -> None:
+        ftle_field = _host(ftle_field)
+        particles_centroid = _host(particles_centroid)
+        if self.dim is None:
+            self.dim = particles_centroid.shape[1]
+        out = os.path.join(self.path, filename + ".mat")
+        if self.grid_shape:
+            if len(self.grid_shape) == 2:
+                nx, ny = self.grid_shape
+                nz = 1
+            elif len(self.grid_shape) == 3:
+                nx, ny, nz = self.grid_shape
+            else:
+                raise ValueError(
+                    f"Invalid grid_shape length {len(self.grid_shape)}. Must be 2 or 3.")
+            f = ftle_field.reshape(nx, ny, nz)
+            c = particles_centroid.reshape(nx, ny, nz, self.dim)
+            data = {"ftle": f, "x": c[..., 0], "y": c[..., 1]}
+            if self.dim == 3:
+                data["z"] = c[..., 2]
+        else:
+            data = {"ftle": ftle_field.ravel(), "x": particles_centroid[:, 0],
+                    "y": particles_centroid[:, 1]}
+            if self.dim == 3:
+                data["z"] = particles_centroid[:, 2]
+        savemat(out, data)
+
+
+def _b64(arr: np.ndarray) -> str:
+    raw = np.ascontiguousarray(arr).tobytes()
+    return base64.b64encode(struct.pack("<Q", len(raw)) + raw).decode("ascii")
+
+
+def _vtk_header(kind: str) -> str:
+    return (f'<?xml version="1.0"?>\n<VTKFile type="{kind}" version="1.0" '
+            f'byte_order="LittleEndian" header_type="UInt64">\n')
+
+
+class VTKWriter(FTLEWriter):
+    """VTK XML ``.vts`` (structured grid) or ``.vtp`` (points) (file_writers.py:167-266).
+
+    Point and cell-free layouts follow the reference: 2D structured points are
+    arranged in Fortran order with z = 0; 3D FTLE values are transposed to the
+    (y, x, z) cartesian order before the Fortran ravel.
+    """
+
+    def write(self, filename: str, ftle_field, particles_centroid) -> None:
+        ftle_field = _host(ftle_field).astype(np.float64)
+        pc = _host(particles_centroid).astype(np.float64)
+        if self.dim is None:
+            self.dim = pc.shape[1]
+        base = os.path.join(self.path, filename)
+        if self.grid_shape is not None:
+            if len(self.grid_shape) == 2:
+                nx, ny = self.grid_shape
+                nz = 1
+                c = pc.reshape(nx, ny, nz, self.dim, order="F")
+                x, y = c[..., 0], c[..., 1]
+                z = np.zeros_like(x)
+                values = ftle_field.ravel(order="F")
+            elif len(self.grid_shape) == 3:
+                nx, ny, nz = self.grid_shape
+                c = pc.reshape(nx, ny, nz, self.dim)
+                x, y, z = c[..., 0], c[..., 1], c[..., 2]
+                values = np.transpose(ftle_field.reshape((nx, ny, nz)), (1, 0, 2)).ravel(order="F")
+            else:
+                raise ValueError(
+                    f"Invalid grid_shape length {len(self.grid_shape)}. Must be 2 or 3.")
+            pts = np.stack([x.ravel(order="F"), y.ravel(order="F"), z.ravel(order="F")], axis=1)
+            ext = f"0 {x.shape[0] - 1} 0 {x.shape[1] - 1} 0 {x.shape[2] - 1}"
+            with open(base + ".vts", "w") as f:
+                f.write(_vtk_header("StructuredGrid"))
+                f.write(f'<StructuredGrid WholeExtent="{ext}">\n<Piece Extent="{ext}">\n')
+                f.write('<PointData Scalars="ftle">\n<DataArray type="Float64" Name="ftle" '
+                        f'format="binary">{_b64(values)}</DataArray>\n</PointData>\n')
+                f.write('<Points>\n<DataArray type="Float64" NumberOfComponents="3" '
+                        f'format="binary">{_b64(pts)}</DataArray>\n</Points>\n')
+                f.write("</Piece>\n</StructuredGrid>\n</VTKFile>\n")
+        else:
+            pts = np.hstack([pc, np.zeros((pc.shape[0], 1))]) if self.dim == 2 else pc
+            n = pts.shape[0]
+            conn = np.arange(n, dtype=np.int64)
+            with open(base + ".vtp", "w") as f:
+                f.write(_vtk_header("PolyData"))
+                f.write(f'<PolyData>\n<Piece NumberOfPoints="{n}" NumberOfVerts="{n}" '
+                        'NumberOfLines="0" NumberOfStrips="0" NumberOfPolys="0">\n')
+                f.write('<PointData Scalars="ftle">\n<DataArray type="Float64" Name="ftle" '
+                        f'format="binary">{_b64(ftle_field.ravel())}</DataArray>\n</PointData>\n')
+                f.write('<Points>\n<DataArray type="Float64" NumberOfComponents="3" '
+                        f'format="binary">{_b64(pts)}</DataArray>\n</Points>\n')
+                f.write('<Verts>\n<DataArray type="Int64" Name="connectivity" format="binary">'
+                        f'{_b64(conn)}</DataArray>\n<DataArray type="Int64" Name="offsets" '
+                        f'format="binary">{_b64(conn + 1)}</DataArray>\n</Verts>\n')
+                f.write("</Piece>\n</PolyData>\n</VTKFile>\n")
+
+
+def create_writer(output_format: str, directory_path: str,
+                  grid_shape: Optional[tuple] = None) -> FTLEWriter:
+    if output_format == "mat":
+        return MatWriter(directory_path, grid_shape)
+    if output_format == "vtk":
+        return VTKWriter(directory_path, grid_shape)
+    raise ValueError(f"Unsupported output format: {output_format}")
+
+
+def read_vtk_xml(path: str) -> dict:
+    """Decode the binary DataArrays of a file written by VTKWriter (for checks)."""
+    import re
+
+    text = open(path).read()
+    out = {}
+    for m in re.finditer(r'<DataArray type="(\w+)"([^>]*)format="binary">([^<]*)</DataArray>',
+                         text):
+        typ, attrs, payload = m.group(1), m.group(2), m.group(3)
+        name = re.search(r'Name="(\w+)"', attrs)
+        ncomp = re.search(r'NumberOfComponents="(\d+)"', attrs)
+        raw = base64.b64decode(payload)
+        n = struct.unpack("<Q", raw[:8])[0]
+        arr = np.frombuffer(raw[8:8 + n], dtype={"Float64": np.float64, "Int64": np.int64}[typ])
+        if ncomp:
+            arr = arr.reshape(-1, int(ncomp.group(1)))
+        out[name.group(1) if name else "points"] = arr
+    return out

@@ -1,0 +1,78 @@
+"""File formats on the host (no GPU): readers and writers mirror pyFTLE's keys,
+orders and shapes (file_readers.py, file_writers.py)."""
+
+import numpy as np
+import pytest
+from scipy.io import loadmat, savemat
+
+from pyftle_b200 import io
+
+
+def test_read_velocity_and_coordinate(tmp_path):
+    savemat(tmp_path / "v2.mat", {"velocity_x": np.array([1.0, 2.0, 3.0]),
+                                  "velocity_y": np.array([4.0, 5.0, 6.0])})
+    v = io.read_velocity(tmp_path / "v2.mat")
+    np.testing.assert_array_equal(v, [[1, 2, 3], [4, 5, 6]])
+    savemat(tmp_path / "c3.mat", {"coordinate_x": np.arange(6.0).reshape(2, 3),
+                                  "coordinate_y": np.ones((2, 3)),
+                                  "coordinate_z": np.zeros((2, 3))})
+    c = io.read_coordinate(tmp_path / "c3.mat")
+    assert c.shape == (3, 6)
+    np.testing.assert_array_equal(c[0], np.arange(6.0))  # C-order ravel
+    savemat(tmp_path / "bad.mat", {"velocity_x": np.zeros(3)})
+    with pytest.raises(ValueError):
+        io.read_velocity(tmp_path / "bad.mat")
+
+
+def test_seed_positions_concatenation_order(tmp_path):
+    d = {"top": [[1.0, 2.0], [3.0, 4.0]], "bottom": [[5.0, 6.0], [7.0, 8.0]],
+         "left": [[9.0, 10.0], [11.0, 12.0]], "right": [[13.0, 14.0], [15.0, 16.0]]}
+    savemat(tmp_path / "s2.mat", d)
+    p = io.read_seed_positions(tmp_path / "s2.mat")
+    np.testing.assert_array_equal(p, np.concatenate([d["left"], d["right"], d["top"],
+                                                     d["bottom"]]))
+    d3 = {k: np.arange(6.0).reshape(2, 3) + i for i, k in
+          enumerate(["top", "bottom", "left", "right", "front", "back"])}
+    savemat(tmp_path / "s3.mat", d3)
+    p3 = io.read_seed_positions(tmp_path / "s3.mat")
+    assert p3.shape == (12, 3)
+    np.testing.assert_array_equal(p3[8:10], d3["front"])
+    with pytest.raises(ValueError):
+        savemat(tmp_path / "bad.mat", {"top": [[1.0, 2.0]]})
+        io.read_seed_positions(tmp_path / "bad.mat")
+
+
+def test_mat_writer_structured_and_unstructured(tmp_path):
+    w = io.create_writer("mat", str(tmp_path / "out"), grid_shape=(3, 2))
+    ftle = np.arange(6.0)
+    cents = np.stack([np.arange(6.0), -np.arange(6.0)], axis=1)
+    w.write("ftle_a", ftle, cents)
+    m = loadmat(tmp_path / "out" / "ftle_a.mat")
+    assert m["ftle"].shape == (3, 2, 1)
+    np.testing.assert_array_equal(m["x"].ravel(), cents[:, 0])
+    u = io.create_writer("mat", str(tmp_path / "out2"))
+    u.write("ftle_b", ftle, np.hstack([cents, np.ones((6, 1))]))
+    m = loadmat(tmp_path / "out2" / "ftle_b.mat")
+    np.testing.assert_array_equal(m["ftle"].ravel(), ftle)
+    assert "z" in m
+    with pytest.raises(ValueError):
+        io.create_writer("hdf5", str(tmp_path))
+
+
+def test_vtk_writer_roundtrip(tmp_path):
+    w = io.create_writer("vtk", str(tmp_path), grid_shape=(4, 3))
+    X, Y = np.meshgrid(np.arange(4.0), np.arange(3.0), indexing="ij")
+    cents = np.stack([X.ravel(order="F"), Y.ravel(order="F")], axis=1)
+    ftle = np.arange(12.0)
+    w.write("ftle_s", ftle, cents)
+    d = io.read_vtk_xml(str(tmp_path / "ftle_s.vts"))
+    np.testing.assert_array_equal(d["ftle"], ftle)
+    assert d["points"].shape == (12, 3) and np.all(d["points"][:, 2] == 0)
+    np.testing.assert_array_equal(d["points"][:, :2], cents)
+    text = open(tmp_path / "ftle_s.vts").read()
+    assert 'WholeExtent="0 3 0 2 0 0"' in text
+    p = io.create_writer("vtk", str(tmp_path))
+    p.write("ftle_p", ftle[:5], np.random.default_rng(0).random((5, 3)))
+    d = io.read_vtk_xml(str(tmp_path / "ftle_p.vtp"))
+    np.testing.assert_array_equal(d["ftle"], ftle[:5])
+    np.testing.assert_array_equal(d["offsets"], np.arange(1, 6))
