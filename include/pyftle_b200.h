@@ -182,6 +182,23 @@ int ftle_window_run_mixed_chunked(const ftle_window *w, void *workspace,
                                   int64_t workspace_bytes, int32_t chunk_steps,
                                   int32_t sort_every, void *stream);
 
+/* ---- closed-form velocity fields -----------------------------------------
+ * The "analytical" interpolator on the device (interpolate.py:765-829 with a
+ * closed-form velocity_fn): FP64 advection of every particle plus the FTLE
+ * epilogue in one launch, with the stage times t0 + i*h (+ h/2, + h).
+ * freeze_time != 0 evaluates the field at t = 0 throughout, which is what
+ * pyFTLE's AnalyticalSolver computes (its interpolator's time never advances,
+ * data_source.py:274-285, interpolate.py:788,812). */
+enum { FTLE_FLOW_DOUBLE_GYRE = 0, FTLE_FLOW_ABC = 1 };
+typedef struct ftle_flow {
+  int32_t kind;       /* FTLE_FLOW_DOUBLE_GYRE (2D) or FTLE_FLOW_ABC (3D) */
+  int32_t reserved;
+  double params[8];   /* double gyre: A, eps, omega; ABC: A, B, C, a, w (A(t) = A + a sin wt) */
+} ftle_flow;
+int ftle_analytic_window_run(const ftle_flow *flow, int32_t integrator, double t0, double h,
+                             int32_t num_steps, int32_t freeze_time, double *positions,
+                             int64_t num_groups, double map_period, double *ftle, void *stream);
+
 /* ---- many windows in one persistent launch -------------------------------
  * Windows that share one packed snapshot series, grid, storage, time mode and
  * integrator, but differ in seed set, start time t0, step h, length and

@@ -45,6 +45,14 @@ class FtleWindow(ctypes.Structure):
                 ("map_period", _f64), ("ftle", _c_dp)]
 
 
+class FtleFlow(ctypes.Structure):
+    """Mirror of ``ftle_flow``."""
+
+    _fields_ = [("kind", _i32), ("reserved", _i32), ("params", _f64 * 8)]
+
+
+FLOW_DOUBLE_GYRE, FLOW_ABC = 0, 1
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "ftle_version": (ctypes.c_int, []),
@@ -74,6 +82,8 @@ SIGNATURES = {
                                                      _i32, _i32, _c_dp]),
     "ftle_window_run_mixed_chunked_static": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32,
                                                             _i32, _c_dp]),
+    "ftle_analytic_window_run": (ctypes.c_int, [ctypes.POINTER(FtleFlow), _i32, _f64, _f64, _i32,
+                                                _i32, _c_dp, _i64, _f64, _c_dp, _c_dp]),
     "ftle_windows_plan_bytes": (ctypes.c_int64, [ctypes.POINTER(FtleWindow), _i32]),
     "ftle_windows_plan": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32, _i32, _c_dp, _i64]),
     "ftle_windows_run_mixed": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32, _c_dp, _i64,

@@ -413,6 +413,136 @@ __global__ void __launch_bounds__(2 * DIM * G)
 }
 
 // ---------------------------------------------------------------------------
+// closed-form velocity fields (the "analytical" interpolator on the device)
+// ---------------------------------------------------------------------------
+
+struct FlowK {
+  int kind;
+  double p[8];
+};
+
+// Double gyre, in the operand order of pyFTLE's example velocity_fn:
+//   f = eps sin(wt) x^2 + (1 - 2 eps sin(wt)) x,  u = -pi A sin(pi f) cos(pi y),
+//   v = pi A cos(pi f) sin(pi y) df/dx.
+// Time-periodic ABC: A(t) = A + a sin(w t), u = A(t) sin z + C cos y,
+//   v = B sin x + A(t) cos z, w = C sin y + B cos x.
+template <int DIM>
+__device__ __forceinline__ void flow_velocity(const FlowK &f, double t, const double *x,
+                                              double *u) {
+  if constexpr (DIM == 2) {
+    const double A = f.p[0], eps = f.p[1], om = f.p[2];
+    const double s = sin(om * t);
+    const double xx = x[0], yy = x[1];
+    const double ff = eps * s * (xx * xx) + (1.0 - 2.0 * eps * s) * xx;
+    const double dfdx = 2.0 * eps * s * xx + (1.0 - 2.0 * eps * s);
+    const double pi = 3.141592653589793;
+    u[0] = -pi * A * sin(pi * ff) * cos(pi * yy);
+    u[1] = pi * A * cos(pi * ff) * sin(pi * yy) * dfdx;
+  } else {
+    const double At = f.p[0] + f.p[3] * sin(f.p[4] * t);
+    const double B = f.p[1], C = f.p[2];
+    u[0] = At * sin(x[2]) + C * cos(x[1]);
+    u[1] = B * sin(x[0]) + At * cos(x[2]);
+    u[2] = C * sin(x[1]) + B * cos(x[0]);
+  }
+}
+
+template <int DIM, int INTEG>
+__device__ __forceinline__ void advect_analytic(const FlowK &f, double t0, double h, int steps,
+                                                int freeze, double *x) {
+  double vprev[DIM];
+  for (int i = 0; i < steps; ++i) {
+    const double t = freeze ? 0.0 : t0 + (double)i * h;
+    if constexpr (INTEG == FTLE_EULER || INTEG == FTLE_AB2) {
+      double v[DIM];
+      flow_velocity<DIM>(f, t, x, v);
+      if (INTEG == FTLE_EULER || i == 0) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) x[a] = x[a] + h * v[a];
+      } else {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) x[a] = x[a] + h * (1.5 * v[a] - 0.5 * vprev[a]);
+      }
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) vprev[a] = v[a];
+    } else {
+      const double hh = 0.5 * h;
+      const double th = freeze ? 0.0 : t + 0.5 * h, tf = freeze ? 0.0 : t + h;
+      double k[DIM], acc[DIM], tmp[DIM];
+      flow_velocity<DIM>(f, t, x, k);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        acc[a] = k[a];
+        tmp[a] = x[a] + hh * k[a];
+      }
+      flow_velocity<DIM>(f, th, tmp, k);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        acc[a] = acc[a] + 2.0 * k[a];
+        tmp[a] = x[a] + hh * k[a];
+      }
+      flow_velocity<DIM>(f, th, tmp, k);
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) {
+        acc[a] = acc[a] + 2.0 * k[a];
+        tmp[a] = x[a] + h * k[a];
+      }
+      flow_velocity<DIM>(f, tf, tmp, k);
+      const double h6 = h / 6.0;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) x[a] = x[a] + h6 * (acc[a] + k[a]);
+    }
+  }
+}
+
+template <int DIM, int INTEG, int G>
+__global__ void __launch_bounds__(2 * DIM * G)
+    analytic_window_kernel(const FlowK f, double t0, double h, int steps, int freeze,
+                           double *positions, long long N, double map_period, double *ftle) {
+  constexpr int K = 2 * DIM;
+  const int tid = threadIdx.x;
+  const int role = tid / G, gl = tid % G;
+  const long long g = (long long)blockIdx.x * G + gl;
+  const bool active = g < N;
+  const long long row = (long long)role * N + g;
+  double x[DIM], x0[DIM];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) x[a] = x0[a] = 0.0;
+  if (active) {
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) x[a] = x0[a] = positions[row * DIM + a];
+    advect_analytic<DIM, INTEG>(f, t0, h, steps, freeze, x);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) positions[row * DIM + a] = x[a];
+  }
+  if (ftle != nullptr) {
+    __shared__ double sx[K][G][DIM];
+    __shared__ double sx0[K][G][DIM];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      sx[role][gl][a] = x[a];
+      sx0[role][gl][a] = x0[a];
+    }
+    __syncthreads();
+    if (tid < G) {
+      const long long gg = (long long)blockIdx.x * G + tid;
+      if (gg < N) {
+        double P[K][DIM];
+        double id[DIM];
+#pragma unroll
+        for (int r = 0; r < K; ++r)
+#pragma unroll
+          for (int a = 0; a < DIM; ++a) P[r][a] = sx[r][tid][a];
+#pragma unroll
+        for (int j = 0; j < DIM; ++j)
+          id[j] = sx0[plus_role(j)][tid][j] - sx0[minus_role(j)][tid][j];
+        ftle[gg] = group_ftle<DIM>(P, id, map_period);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // per-step kernels (compatibility path of the Integrator / Interpolator API)
 // ---------------------------------------------------------------------------
 
@@ -869,6 +999,44 @@ int ftle_from_positions(int32_t dim, const double *positions, const double *init
   DIM_DISPATCH(dim, ftle_from_positions_kernel, positions, initial_deltas, num_groups,
                map_period, out);
   return check_launch("ftle_from_positions_kernel");
+}
+
+int ftle_analytic_window_run(const ftle_flow *flow, int32_t integrator, double t0, double h,
+                             int32_t num_steps, int32_t freeze_time, double *positions,
+                             int64_t num_groups, double map_period, double *ftle, void *stream) {
+  if (!flow) return fail_invalid("flow descriptor is NULL");
+  int dim;
+  if (flow->kind == FTLE_FLOW_DOUBLE_GYRE)
+    dim = 2;
+  else if (flow->kind == FTLE_FLOW_ABC)
+    dim = 3;
+  else
+    return fail_invalid("unknown flow kind %d", flow->kind);
+  if (integrator < FTLE_EULER || integrator > FTLE_RK4)
+    return fail_invalid("unknown integrator %d", integrator);
+  if (num_steps < 0 || num_groups < 0) return fail_invalid("sizes must be >= 0");
+  if (ftle && !(map_period > 0.0) && !(map_period < 0.0))
+    return fail_invalid("map_period must be non-zero");
+  if (num_groups == 0) return FTLE_OK;
+  if (!positions) return fail_invalid("positions are required");
+  FlowK f;
+  f.kind = flow->kind;
+  for (int i = 0; i < 8; ++i) f.p[i] = flow->params[i];
+  cudaStream_t st = as_stream(stream);
+#define AN(D, I, G)                                                                       \
+  analytic_window_kernel<D, I, G><<<(unsigned)((num_groups + G - 1) / G), 2 * D * G, 0, st>>>( \
+      f, t0, h, num_steps, freeze_time, positions, num_groups, map_period, ftle)
+  if (dim == 2) {
+    if (integrator == FTLE_EULER) AN(2, FTLE_EULER, 64);
+    else if (integrator == FTLE_AB2) AN(2, FTLE_AB2, 64);
+    else AN(2, FTLE_RK4, 64);
+  } else {
+    if (integrator == FTLE_EULER) AN(3, FTLE_EULER, 32);
+    else if (integrator == FTLE_AB2) AN(3, FTLE_AB2, 32);
+    else AN(3, FTLE_RK4, 32);
+  }
+#undef AN
+  return check_launch("analytic_window_kernel");
 }
 
 }  // extern "C"

@@ -23,6 +23,8 @@ Outputs (all float64, small):
   windows_2d.npz   FTLESolver.run over double-gyre windows (Euler/AB2/RK4,
                    forward and backward time): final positions and FTLE
   windows_3d.npz   FTLESolver.run over ABC windows on a cubic grid
+  analytical.npz   FTLESolver.run with AnalyticalBatchSource / AnalyticalInterpolator
+                   (pyFTLE's notebook double gyre; the reference evaluates it at t = 0)
 """
 
 from __future__ import annotations
@@ -276,6 +278,36 @@ def gen_windows_3d():
     np.savez_compressed(os.path.join(HERE, "windows_3d.npz"), **res)
 
 
+def gen_analytical():
+    from pyftle.data_source import AnalyticalBatchSource
+    from pyftle.ftle_solver import FTLESolver
+    from pyftle.integrate import create_integrator
+    from pyftle.interpolate import create_interpolator
+    from pyftle.particles import NeighboringParticles
+    from pyftle_b200 import flows
+
+    A, EPS, OMEGA = 0.1, 0.25, 2.0  # the notebook's constants
+
+    def velocity_fn(t, coordinates):
+        return flows.double_gyre_velocity(t, coordinates, A=A, eps=EPS, omega=OMEGA)
+
+    pos = flows.seeds_2d(flows.centroid_grid_2d(15, 8, (0.2, 1.8), (0.2, 0.8)), 1e-3)
+    res = {"positions": pos}
+    for name in ("euler", "rk4"):
+        for dt in (0.01, -0.01):
+            T = 0.1
+            p = int(T / abs(dt)) + 1
+            times = np.arange(p) * dt
+            src = AnalyticalBatchSource(velocity_fn, NeighboringParticles(pos.copy()), dt, times)
+            integ = create_integrator(name, create_interpolator("analytical",
+                                                              velocity_fn=velocity_fn))
+            solver = FTLESolver(src, integ)
+            f = solver.run()
+            res[f"{name}_{dt}_ftle"] = np.asarray(f)
+            res[f"{name}_{dt}_pos"] = solver.particles.positions.copy()
+    np.savez(os.path.join(HERE, "analytical.npz"), **res)
+
+
 def main():
     tmp = stage_reference()
     try:
@@ -286,6 +318,7 @@ def main():
         gen_integrate()
         gen_windows_2d()
         gen_windows_3d()
+        gen_analytical()
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
     for f in sorted(os.listdir(HERE)):
