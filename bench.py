@@ -49,7 +49,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["abc", "batched"], default="abc",
+    p.add_argument("--workload", choices=["abc", "batched", "gyre", "abc256"], default="abc",
                    help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
                         "turbulence windows in one persistent launch")
     p.add_argument("--precision", choices=["fx15", "fp16", "bf16", "fp64"], default="fx15")
@@ -58,6 +58,7 @@ def parse_args():
     p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
     p.add_argument("--h", type=float, default=0.02)
     p.add_argument("--T", type=float, default=8.0)
+    p.add_argument("--windows", type=int, default=32, help="abc256: number of windows")
     p.add_argument("--urms", type=float, default=0.02,
                    help="batched workload: rms speed of the turbulence field")
     p.add_argument("--chunk-steps", type=int, default=50,
@@ -553,12 +554,177 @@ def run_batched(args):
     return 0
 
 
+def run_gyre(args):
+    """The 2D double gyre of the reference's own CPU case, in both time modes.
+
+    512 x 256 grid over [0,2] x [0,1], 201 snapshots at dt = 0.05 (A = 0.1, eps = 0.25,
+    omega = 2 pi/10), 400 x 200 centroids x 4 neighbours at delta = 1e-3.
+      hold:  the reference's semantics (step i holds snapshot i, h = dt = 0.05, 201
+             steps) -- plain FP64, bit-exact with pyFTLE; the reference's CPU path
+             timed on the same workload on the host cores.
+      blend: RK4 h = 0.01 over T = 10 (1000 steps) on time-blended snapshots --
+             the chosen FX15 path vs plain FP64.
+    """
+    import torch
+
+    from oracle import ref_driver
+    from pyftle_b200 import SnapshotSeries, flows, run_window
+    from pyftle_b200.interpolate import GridSpec
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    shape = (512, 256)
+    pts = flows.grid_points_2d(*shape, (0.0, 2.0), (0.0, 1.0))
+    dt = 0.05
+    snaps = flows.double_gyre_snapshots(pts, np.arange(201) * dt)
+    pos0 = flows.seeds_2d(flows.centroid_grid_2d(400, 200, (0.005, 1.995), (0.005, 0.995)),
+                          1e-3)
+    grid = GridSpec.from_points(pts, shape)
+    d_snaps = torch.from_numpy(snaps).cuda()
+    d_pos0 = torch.from_numpy(pos0).cuda()
+    N = pos0.shape[0] // 4
+    out = {"workload": "2D double gyre 512x256, 201 snapshots dt=0.05, 400x200 centroids x 4 "
+                       "(delta 1e-3)"}
+
+    def timed(series, kw, reps):
+        p = d_pos0.clone()
+        f = run_window(series, p, **kw)
+        ts = []
+        for _ in range(reps):
+            p.copy_(d_pos0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            f = run_window(series, p, ftle_out=f, **kw)
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return min(ts), f, p
+
+    s64 = SnapshotSeries(grid, d_snaps, precision="fp64")
+    hold = dict(integrator="rk4", time_mode="hold", h=dt, num_steps=201, snapshot_dt=dt)
+    ms, f_hold, p_hold = timed(s64, hold, max(args.steps, 3))
+    ps = 4 * N * 201
+    out["hold_fp64"] = {"particle_steps_per_s": ps / (ms / 1e3), "ms_per_window": ms,
+                        "fields_per_s": 1e3 / ms}
+    # reference CPU path on a sample of the same window (its own ginterp, HOLD RK4)
+    sample_groups, sample_steps = 20000, 10
+    sel = np.concatenate([np.arange(r * N, r * N + sample_groups) for r in range(4)])
+    r = ref_driver.time_reference(snaps[:sample_steps], pts, shape, pos0[sel], dt)
+    out["hold_reference_cpu"] = {"particle_steps_per_s": r["value"], "cores": r["cores"],
+                                 "kind": r["kind"],
+                                 "sample": f"{sample_groups} groups x 4 x {sample_steps} steps "
+                                           f"per worker, {r['cores']} workers"}
+    out["hold_speedup_gpu_vs_reference_cpu"] = out["hold_fp64"]["particle_steps_per_s"] / r["value"]
+    # bit-exactness spot check of the GPU HOLD window against the compiled reference path
+    g = ref_driver.load_ginterp()
+    if g is not None:
+        chk = np.concatenate([np.arange(r_ * N, r_ * N + 500) for r_ in range(4)])
+        it = ref_driver.RefGridInterpolator(g, shape)
+        pr = pos0[chk].copy()
+        for sidx in range(201):
+            it.update(snaps[sidx], pts)
+            ref_driver.rk4_step(it, pr, dt)
+        pg = p_hold.cpu().numpy()[chk]
+        out["hold_positions_bitexact_vs_reference_500_groups"] = bool(np.array_equal(pg, pr))
+    # BLEND, 1000 steps of h = 0.01
+    blend = dict(integrator="rk4", time_mode="blend", h=0.01, num_steps=1000, snapshot_dt=dt,
+                 map_period=10.0)
+    ms64, f64, _ = timed(s64, blend, max(args.steps, 2))
+    sfx = SnapshotSeries(grid, d_snaps, precision="fx15")
+    msfx, ffx, _ = timed(sfx, dict(blend, chunk_steps=100, sort_every=1), max(args.steps, 3))
+    ps = 4 * N * 1000
+    err = float(torch.linalg.vector_norm(ffx - f64) / torch.linalg.vector_norm(f64))
+    out["blend_fp64"] = {"particle_steps_per_s": ps / (ms64 / 1e3), "ms_per_window": ms64}
+    out["blend_fx15"] = {"particle_steps_per_s": ps / (msfx / 1e3), "ms_per_window": msfx,
+                         "ftle_rel_err_l2_vs_fp64": err,
+                         "speedup_vs_fp64": ms64 / msfx}
+    print(json.dumps({"metric": METRIC + " (2D double gyre)", **out}), flush=True)
+    return 0
+
+
+def run_abc256(args):
+    """Large 3D case: ABC on a 256^3 periodic grid, 64 FX15 snapshots over one period,
+    512 x 512 x 256 centroids x 6 neighbours (402.7M particles, delta 1e-3) read from
+    one shared seed buffer, windows of length U[2, 12] (h = 0.02, random start times),
+    all in one persistent launch with the FP64 Cauchy-Green / lambda_max epilogue.
+    One timed replay after a one-window warm-up (the full batch runs for minutes)."""
+    import torch
+
+    from pyftle_b200 import SnapshotSeries, flows, run_window
+    from pyftle_b200.batch import WindowBatch, WindowSpecRun
+    from pyftle_b200.interpolate import GridSpec
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rng = np.random.default_rng(256)
+    n, S = 256, 64
+    L = 2 * math.pi
+    ax = flows.periodic_axis(n, L)
+    dt = L / S
+    snaps = flows.abc_snapshots_device(ax, ax, ax, np.arange(S) * dt)
+    grid = GridSpec(shape=(n, n, n), origin=(0.0,) * 3, spacing=(ax[1],) * 3, periodic=True)
+    series = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+    del snaps
+    torch.cuda.empty_cache()
+    # seeds: 512 x 512 x 256 centroids (meshgrid "xy" order), role-blocked, on the device
+    cx = (torch.arange(512, dtype=torch.float64, device="cuda") + 0.5) * (L / 512)
+    cz = (torch.arange(256, dtype=torch.float64, device="cuda") + 0.5) * (L / 256)
+    Y, X, Z = torch.meshgrid(cx, cx, cz, indexing="ij")
+    cents = torch.stack((X.reshape(-1), Y.reshape(-1), Z.reshape(-1)), dim=1)
+    del X, Y, Z
+    d = 1e-3
+    offs = torch.tensor([[-d, 0, 0], [d, 0, 0], [0, d, 0], [0, -d, 0], [0, 0, d], [0, 0, -d]],
+                        dtype=torch.float64, device="cuda")
+    seeds = torch.cat([cents + offs[r] for r in range(6)]).contiguous()
+    del cents
+    N = seeds.shape[0] // 6
+    h = 0.02
+    wins = []
+    for i in range(args.windows):
+        steps = int(round(rng.uniform(2.0, 12.0) / h))
+        wins.append(WindowSpecRun(seeds, float(rng.uniform(0.0, L)), h, steps,
+                                  keep_positions=True))
+    warm = WindowBatch(series, [WindowSpecRun(seeds, 0.0, h, 5, keep_positions=True)],
+                       snapshot_dt=dt)
+    warm.run()
+    del warm
+    batch = WindowBatch(series, wins, snapshot_dt=dt)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    batch.run()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    ps = sum(6 * N * w.num_steps for w in wins)
+    # FP64 check on 1/256 of the groups of window 0
+    m = N // 256
+    sub = torch.cat([seeds[r * N:r * N + m] for r in range(6)]).contiguous()
+    s64 = SnapshotSeries(grid, flows.abc_snapshots_device(ax, ax, ax, np.arange(S) * dt),
+                         precision="fp64", periodic_time=True)
+    w0 = wins[0]
+    f64 = run_window(s64, sub.clone(), integrator="rk4", time_mode="blend", h=h,
+                     num_steps=w0.num_steps, t0=w0.t0, snapshot_dt=dt)
+    err = float(torch.linalg.vector_norm(w0.ftle[:m] - f64) / torch.linalg.vector_norm(f64))
+    print(json.dumps({
+        "metric": METRIC + " (large 3D batch)", "value": ps / (ms / 1e3), "unit": UNIT,
+        "ms_batch": ms, "windows": len(wins), "particles_per_window": 6 * N,
+        "particle_steps": ps, "ftle_fields_per_s": len(wins) / (ms / 1e3),
+        "ftle_rel_err_l2_window0_subset_vs_fp64": err,
+        "config": {"workload": "ABC 256^3 periodic, 64 FX15 snapshots/period, 512x512x256 "
+                               "centroids x 6, windows U[2,12] h=0.02, one persistent launch, "
+                               "shared read-only seeds"}}), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.workload == "abc256" and args.impl != "reference":
+        return run_abc256(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "gyre":
+        return run_gyre(args)
     return run_ours(args)
 
 

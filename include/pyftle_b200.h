@@ -39,6 +39,7 @@ enum {
 
 enum { FTLE_EULER = 0, FTLE_AB2 = 1, FTLE_RK4 = 2 };    /* integrate.py:372-376 keys */
 enum { FTLE_HOLD = 0, FTLE_BLEND = 1 };                 /* time modes */
+enum { FTLE_KEEP_POSITIONS = 1 };                       /* ftle_window.flags */
 /* Snapshot storage.  FTLE_FX15: 15-bit fixed point per component over the
  * series' value range (uniform absolute error range/65534; decoded by one
  * byte permute into an FP32 in [0.5, 1)). */
@@ -74,7 +75,8 @@ typedef struct ftle_window {
   double t0;               /* BLEND: time of step 0 */
   double h;                /* step; negative for backward time */
   int32_t num_steps;
-  int32_t reserved;
+  int32_t flags;           /* FTLE_KEEP_POSITIONS: read the seeds, do not write final
+                              positions back (windows may then share one seed buffer) */
   double *positions;       /* (K*N, dim) in/out, role-blocked */
   int64_t num_groups;      /* N */
   double map_period;       /* T in FTLE = log(sqrt(lambda_max))/T; reference: (steps-1)*|dt| */

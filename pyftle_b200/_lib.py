@@ -41,7 +41,7 @@ class FtleWindow(ctypes.Structure):
                 ("storage", _i32), ("time_mode", _i32), ("periodic_time", _i32),
                 ("snapshot_t0", _f64), ("snapshot_dt", _f64), ("first_snapshot", _i32),
                 ("integrator", _i32), ("t0", _f64), ("h", _f64), ("num_steps", _i32),
-                ("reserved", _i32), ("positions", _c_dp), ("num_groups", _i64),
+                ("flags", _i32), ("positions", _c_dp), ("num_groups", _i64),
                 ("map_period", _f64), ("ftle", _c_dp)]
 
 
@@ -52,6 +52,7 @@ class FtleFlow(ctypes.Structure):
 
 
 FLOW_DOUBLE_GYRE, FLOW_ABC = 0, 1
+KEEP_POSITIONS = 1
 
 # name -> (restype, argtypes)
 SIGNATURES = {

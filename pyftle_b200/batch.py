@@ -43,6 +43,7 @@ class WindowSpecRun:
     map_period: Optional[float] = None
     ftle: Optional[torch.Tensor] = None
     first_snapshot: int = 0  # HOLD windows: snapshot used by step 0
+    keep_positions: bool = False  # read-only seeds (windows may share one buffer)
 
 
 @dataclass(frozen=True)
@@ -70,7 +71,7 @@ class WindowBatch:
             mp = w.map_period if w.map_period is not None else w.num_steps * abs(w.h)
             arr[i] = window_descriptor(series, w.positions, w.ftle, h=w.h, num_steps=w.num_steps,
                                        map_period=mp, t0=w.t0, first_snapshot=w.first_snapshot,
-                                       **self.kw)
+                                       keep_positions=w.keep_positions, **self.kw)
         self.desc = arr
         self.count = len(self.windows)
         self.graph: Optional[torch.cuda.CUDAGraph] = None

@@ -97,6 +97,7 @@ int window_to_kernel(const ftle_window *w, WinK *k) {
   k->positions = w->positions;
   k->N = w->num_groups;
   k->ftle = w->ftle;
+  k->keep_positions = (w->flags & FTLE_KEEP_POSITIONS) ? 1 : 0;
   return FTLE_OK;
 }
 

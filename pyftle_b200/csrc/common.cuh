@@ -39,6 +39,7 @@ struct WinK {
   double *positions;
   long long N;
   double *ftle;
+  int keep_positions;  // FTLE_KEEP_POSITIONS: do not write final positions
 };
 
 // Validates an ftle_window and converts it to kernel constants.

@@ -253,6 +253,8 @@ struct WinVar {
   double *ftle;
   long long N;
   int num_steps, first_snapshot;
+  int keep_positions;
+  int reserved;
 };
 
 __device__ __forceinline__ WinVar winvar_of(const MixK &m) {
@@ -265,6 +267,8 @@ __device__ __forceinline__ WinVar winvar_of(const MixK &m) {
   v.N = m.w.N;
   v.num_steps = m.w.num_steps;
   v.first_snapshot = m.w.first_snapshot;
+  v.keep_positions = m.w.keep_positions;
+  v.reserved = 0;
   return v;
 }
 
@@ -793,11 +797,13 @@ __device__ __forceinline__ void group_finish(const MixK &m, const WinVar &v, lon
 #pragma unroll
   for (int a = 0; a < DIM; ++a)
     c[a] = m.w.g.periodic ? st.c[a] + (double)st.wraps[a] * m.period[a] : st.c[a];
+  if (!v.keep_positions) {
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+    for (int k = 0; k < K; ++k)
 #pragma unroll
-    for (int a = 0; a < DIM; ++a)
-      v.positions[((long long)k * N + g) * DIM + a] = c[a] + (double)st.d[k][a];
+      for (int a = 0; a < DIM; ++a)
+        v.positions[((long long)k * N + g) * DIM + a] = c[a] + (double)st.d[k][a];
+  }
   if (v.ftle != nullptr) {
     double J[DIM][DIM];
 #pragma unroll
@@ -1351,6 +1357,8 @@ int ftle_windows_plan(const ftle_window *windows, int32_t count, int32_t order, 
     wins[i].N = w.num_groups;
     wins[i].num_steps = w.num_steps;
     wins[i].first_snapshot = w.first_snapshot;
+    wins[i].keep_positions = (w.flags & FTLE_KEEP_POSITIONS) ? 1 : 0;
+    wins[i].reserved = 0;
   }
   // order 1: longest windows first (work items of long windows are scheduled before short
   // ones so the tail of the persistent launch is short); order 0: as given.

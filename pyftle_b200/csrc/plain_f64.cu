@@ -383,8 +383,10 @@ __global__ void __launch_bounds__(2 * DIM * G)
 #pragma unroll
     for (int a = 0; a < DIM; ++a) x[a] = x0[a] = w.positions[row * DIM + a];
     advect<DIM, MODE, INTEG>(w, x);
+    if (!w.keep_positions) {
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) w.positions[row * DIM + a] = x[a];
+      for (int a = 0; a < DIM; ++a) w.positions[row * DIM + a] = x[a];
+    }
   }
   if (w.ftle != nullptr) {  // uniform across the block
     __shared__ double sx[K][G][DIM];

@@ -149,6 +149,23 @@ def abc_snapshots(x: np.ndarray, y: np.ndarray, z: np.ndarray, times, A=ABC_A, B
     return out.reshape(S, 3, nx * ny * nz)
 
 
+def abc_snapshots_device(x, y, z, times, A=ABC_A, B=ABC_B, C=ABC_C, device="cuda"):
+    """``abc_snapshots`` built on the device as a (S, 3, nx*ny*nz) float64 tensor."""
+    import torch
+
+    tx = torch.as_tensor(np.asarray(x), dtype=torch.float64, device=device)
+    ty = torch.as_tensor(np.asarray(y), dtype=torch.float64, device=device)
+    tz = torch.as_tensor(np.asarray(z), dtype=torch.float64, device=device)
+    nx, ny, nz = len(tx), len(ty), len(tz)
+    out = torch.empty((len(times), 3, ny, nx, nz), dtype=torch.float64, device=device)
+    for s, t in enumerate(times):
+        At = A + 0.1 * math.sin(float(t))
+        out[s, 0] = (At * torch.sin(tz))[None, None, :] + (C * torch.cos(ty))[:, None, None]
+        out[s, 1] = (B * torch.sin(tx))[None, :, None] + (At * torch.cos(tz))[None, None, :]
+        out[s, 2] = (C * torch.sin(ty))[:, None, None] + (B * torch.cos(tx))[None, :, None]
+    return out.reshape(len(times), 3, nx * ny * nz)
+
+
 # ----------------------------------------------------------------------------
 # 2D random-Fourier turbulence
 # ----------------------------------------------------------------------------

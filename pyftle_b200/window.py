@@ -73,7 +73,8 @@ class SnapshotSeries:
 def window_descriptor(series: SnapshotSeries, positions: torch.Tensor, ftle: Optional[torch.Tensor],
                       *, integrator: str, time_mode: str, h: float, num_steps: int,
                       map_period: float, t0: float = 0.0, first_snapshot: int = 0,
-                      snapshot_t0: float = 0.0, snapshot_dt: float = 1.0) -> _lib.FtleWindow:
+                      snapshot_t0: float = 0.0, snapshot_dt: float = 1.0,
+                      keep_positions: bool = False) -> _lib.FtleWindow:
     dim = series.grid.dim
     K = 2 * dim
     if positions.dtype != torch.float64 or not positions.is_cuda or not positions.is_contiguous():
@@ -94,6 +95,7 @@ def window_descriptor(series: SnapshotSeries, positions: torch.Tensor, ftle: Opt
     w.t0 = float(t0)
     w.h = float(h)
     w.num_steps = int(num_steps)
+    w.flags = _lib.KEEP_POSITIONS if keep_positions else 0
     w.positions = positions.data_ptr()
     w.num_groups = positions.shape[0] // K
     w.map_period = float(map_period)
@@ -107,8 +109,8 @@ def run_window(series: SnapshotSeries, positions: torch.Tensor, *, integrator: s
                snapshot_t0: float = 0.0, snapshot_dt: Optional[float] = None,
                ftle_out: Optional[torch.Tensor] = None, with_ftle: bool = True,
                stream: Optional[torch.cuda.Stream] = None, chunk_steps: Optional[int] = None,
-               sort_every: int = 1,
-               workspace: Optional[torch.Tensor] = None) -> Optional[torch.Tensor]:
+               sort_every: int = 1, workspace: Optional[torch.Tensor] = None,
+               keep_positions: bool = False) -> Optional[torch.Tensor]:
     """Advect ``positions`` (in place) through one window; return the FTLE field.
 
     Mixed precision only: ``chunk_steps`` splits the window into launches of that
@@ -133,7 +135,7 @@ def run_window(series: SnapshotSeries, positions: torch.Tensor, *, integrator: s
     w = window_descriptor(series, positions, ftle, integrator=integrator, time_mode=time_mode,
                           h=h, num_steps=num_steps, map_period=map_period, t0=t0,
                           first_snapshot=first_snapshot, snapshot_t0=snapshot_t0,
-                          snapshot_dt=snapshot_dt)
+                          snapshot_dt=snapshot_dt, keep_positions=keep_positions)
     if series.storage == _lib.F64:
         _lib.call("ftle_window_run_f64", w, stream_ptr(stream))
     elif chunk_steps is None or n == 0:

@@ -409,3 +409,16 @@ def test_mixed_chunked_2d_nonperiodic_equals_single_launch():
     f2 = run_window(series, p2, chunk_steps=9, sort_every=1, **kw)
     np.testing.assert_array_equal(host(p2), host(p1))
     np.testing.assert_array_equal(host(f2), host(f1))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fx15"])
+def test_keep_positions_leaves_seeds_and_same_ftle(precision):
+    shape, pts, snaps, pos = _blend_case_2d(30, 15)
+    series = SnapshotSeries(GridSpec.from_points(pts, shape), snaps, precision=precision)
+    kw = dict(integrator="rk4", time_mode="blend", h=0.013, num_steps=40, snapshot_dt=0.05)
+    p1 = torch.as_tensor(pos, device="cuda")
+    f1 = run_window(series, p1, **kw)
+    p2 = torch.as_tensor(pos, device="cuda")
+    f2 = run_window(series, p2, keep_positions=True, **kw)
+    np.testing.assert_array_equal(host(p2), pos)
+    np.testing.assert_array_equal(host(f2), host(f1))
