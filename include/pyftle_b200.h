@@ -231,6 +231,69 @@ int ftle_windows_run_mixed(const ftle_window *windows, int32_t count, void *devi
 int ftle_window_run_mixed_chunked_static(const ftle_window *w, int32_t chunk_steps,
                                          int32_t sort_every, void *stream);
 
+/* ---- flow-map surrogate MLP ------------------------------------------------
+ * Kernels of the learned flow-map surrogate (Fourier features of (x0, y0, t0)
+ * -> SiLU MLP -> displacement over a fixed T), which replaces advection for
+ * sliding windows, with RK4 (ftle_window_run_*) as its judge and fallback.
+ * No counterpart in the reference (it has no learned path); the nearest
+ * interface is the advection it replaces, ftle_solver.py:116-149.
+ * All matrices are row-major BF16 (2 bytes per element) unless named FP32;
+ * a "transposed" operand stores element (r, k) at src[k*ld + r].
+ * M, N multiples of 8, K a multiple of 64, operands 16-byte aligned,
+ * leading dimensions multiples of 8.  `error_word` (device int32) is set to 1
+ * when a tensor-core wait times out; the call's status reports launch errors. */
+
+/* C[M x N] (+)= A[M x K] * B[N x K]^T, FP32 C; splits > 1 splits K (C accumulated). */
+int ftle_mlp_gemm(const void *A, int32_t lda, int32_t a_trans, const void *B, int32_t ldb,
+                  int32_t b_trans, float *C, int32_t ldc, int32_t M, int32_t N, int32_t K,
+                  int32_t splits, int32_t accumulate, int32_t *error_word, void *stream);
+/* Z = X W^T + b; activation != 0: Z (FP32, may be NULL) and H = silu(Z) (BF16);
+ * activation == 0: Z = X W^T + b only (FP32). */
+int ftle_mlp_linear(const void *X, int32_t ldx, const void *W, int32_t ldw, const float *bias,
+                    int32_t M, int32_t N, int32_t K, int32_t activation, float *Z, int32_t ldz,
+                    void *H, int32_t ldh, int32_t *error_word, void *stream);
+/* G = (A B^T) * silu'(Zin) (BF16); colsum (FP32, may be NULL) += column sums of G. */
+int ftle_mlp_gemm_dsilu(const void *A, int32_t lda, int32_t a_trans, const void *B, int32_t ldb,
+                        int32_t b_trans, int32_t M, int32_t N, int32_t K, const float *Zin,
+                        int32_t ldz, void *G, int32_t ldg, float *colsum, int32_t *error_word,
+                        void *stream);
+/* Features of points (n x 3 FP64: x, y, t) for freq (num_freq x 4 FP32: kx, ky,
+ * kt, phase): [sin | cos] (n x 2*num_freq BF16), and their d/dx, d/dy (may be NULL). */
+int ftle_mlp_features(const double *points, int64_t n, const float *freq, int32_t num_freq,
+                      void *features, void *tangent_x, void *tangent_y, void *stream);
+/* MSE loss over `outs` (<= 4) columns: dy = 2 (y - target) / n (BF16, lddy columns,
+ * padding zero), dbias += column sums of dy, *loss += mean squared error. */
+int ftle_mlp_mse_grad(const float *y, int32_t ldy, const float *target, int32_t outs, int64_t n,
+                      void *dy, int32_t lddy, float *dbias, float *loss, void *stream);
+/* Adam step `step` (1-based) with decoupled weight decay on FP32 w; writes the
+ * BF16 copy w_bf16 and zeroes g. */
+int ftle_mlp_adam(float *w, float *g, float *m, float *v, void *w_bf16, int64_t n, float lr,
+                  float beta1, float beta2, float eps, int32_t step, float weight_decay,
+                  void *stream);
+/* FTLE (FP64) of x -> x + scale * y(x) from the tangents jx = dy/dx0, jy = dy/dy0
+ * (FP32 rows, columns 0 and 1), as ftle_from_jacobian for 2D. */
+int ftle_mlp_jacobian_ftle(const float *jx, const float *jy, int32_t ld, int64_t n, double scale,
+                           double T, double *ftle, void *stream);
+/* out (n x 2 FP64) = points[:, :2] + scale * y[:, :2]. */
+int ftle_mlp_apply_displacement(const double *points, const float *y, int32_t ldy, int64_t n,
+                                double scale, double *out, void *stream);
+
+/* Fused surrogate inference for the fixed shape 32 frequencies (64 features) ->
+ * 4 x 256 SiLU -> 2 outputs: one persistent launch evaluates the network and its
+ * two Jacobian tangents per seed and writes the FTLE (as ftle_mlp_jacobian_ftle)
+ * and/or the predicted end positions.  Weights are first packed into the
+ * kernel's chunk images (ftle_surrogate_packed_bytes() bytes, 16-byte aligned)
+ * from the BF16 matrices w0 (256 x 64), w1..w3 (256 x 256) and w4 (>= 16 rows x
+ * 256; rows 2..15 zero).  bias: 4*256 + 16 FP32 (hidden layers, then the output
+ * layer padded to 16).  points: n x 2 FP64 seed positions, all at start time t0.
+ * No counterpart in the reference (it stands for ftle_solver.py:116-161). */
+int64_t ftle_surrogate_packed_bytes(void);
+int ftle_surrogate_pack(const void *w0, const void *w1, const void *w2, const void *w3,
+                        const void *w4, void *packed, void *stream);
+int ftle_surrogate_ftle(const double *points, int64_t n, double t0, const void *packed,
+                        const float *bias, const float *freq, double out_scale, double T,
+                        double *ftle, double *end_positions, int32_t *error_word, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

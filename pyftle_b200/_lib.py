@@ -24,7 +24,7 @@ STORAGE_CODES = {"fp64": F64, "fp16": F16, "bf16": BF16, "fx15": FX15}
 TIME_MODES = {"hold": HOLD, "blend": BLEND}
 
 _c_dp = ctypes.c_void_p  # device pointers travel as plain addresses
-_i32, _i64, _f64 = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+_i32, _i64, _f64, _f32 = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_float
 
 
 class FtleGrid(ctypes.Structure):
@@ -89,6 +89,26 @@ SIGNATURES = {
     "ftle_windows_plan": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32, _i32, _c_dp, _i64]),
     "ftle_windows_run_mixed": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _i32, _c_dp, _i64,
                                               _i32, _c_dp]),
+    # flow-map surrogate MLP (BF16 tensor-core kernels)
+    "ftle_mlp_gemm": (ctypes.c_int, [_c_dp, _i32, _i32, _c_dp, _i32, _i32, _c_dp, _i32, _i32,
+                                     _i32, _i32, _i32, _i32, _c_dp, _c_dp]),
+    "ftle_mlp_linear": (ctypes.c_int, [_c_dp, _i32, _c_dp, _i32, _c_dp, _i32, _i32, _i32, _i32,
+                                       _c_dp, _i32, _c_dp, _i32, _c_dp, _c_dp]),
+    "ftle_mlp_gemm_dsilu": (ctypes.c_int, [_c_dp, _i32, _i32, _c_dp, _i32, _i32, _i32, _i32,
+                                           _i32, _c_dp, _i32, _c_dp, _i32, _c_dp, _c_dp, _c_dp]),
+    "ftle_mlp_features": (ctypes.c_int, [_c_dp, _i64, _c_dp, _i32, _c_dp, _c_dp, _c_dp, _c_dp]),
+    "ftle_mlp_mse_grad": (ctypes.c_int, [_c_dp, _i32, _c_dp, _i32, _i64, _c_dp, _i32, _c_dp,
+                                         _c_dp, _c_dp]),
+    "ftle_mlp_adam": (ctypes.c_int, [_c_dp, _c_dp, _c_dp, _c_dp, _c_dp, _i64, _f32, _f32, _f32,
+                                     _f32, _i32, _f32, _c_dp]),
+    "ftle_mlp_jacobian_ftle": (ctypes.c_int, [_c_dp, _c_dp, _i32, _i64, _f64, _f64, _c_dp,
+                                              _c_dp]),
+    "ftle_mlp_apply_displacement": (ctypes.c_int, [_c_dp, _c_dp, _i32, _i64, _f64, _c_dp,
+                                                   _c_dp]),
+    "ftle_surrogate_packed_bytes": (ctypes.c_int64, []),
+    "ftle_surrogate_pack": (ctypes.c_int, [_c_dp, _c_dp, _c_dp, _c_dp, _c_dp, _c_dp, _c_dp]),
+    "ftle_surrogate_ftle": (ctypes.c_int, [_c_dp, _i64, _f64, _c_dp, _c_dp, _c_dp, _f64, _f64,
+                                           _c_dp, _c_dp, _c_dp, _c_dp]),
 }
 
 _lock = threading.Lock()

@@ -31,8 +31,10 @@ SOURCES = {
     "plain_f64.cu": ["-fmad=false"],
     "mixed.cu": [],
     "no_alloc.cu": [],
+    "mlp.cu": [],
+    "mlp_fused.cu": [],
 }
-HEADERS = ["common.cuh"]
+HEADERS = ["common.cuh", "umma.cuh"]
 
 
 def nvcc() -> str:

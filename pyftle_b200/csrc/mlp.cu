@@ -1,0 +1,583 @@
+// mlp.cu -- BF16 tensor-core (tcgen05 / TMEM) kernels of the flow-map surrogate MLP.
+//
+// GEMM: C[M x N] (+)= A[M x K] * B[N x K]^T, BF16 operands, FP32 accumulation in
+// tensor memory.  One CTA (4 warps) owns a 128 x NT tile (NT <= 256) of C:
+//   * operands are staged in shared memory in the no-swizzle K-major "core
+//     matrix" layout (8 rows x 16 bytes per core matrix, K chunks 128 B apart,
+//     8-row groups KC*16 B apart), two stages deep so the loads of chunk c+1
+//     overlap the MMAs of chunk c; the loader reads A/B either row-major or
+//     transposed, so every product of training (X W^T, dZ W, dZ^T X) and of the
+//     Jacobian tangents runs through this one kernel; rows past M (or N) load as 0;
+//   * one elected thread issues tcgen05.mma (kind::f16, M = 128, N = NT, K = 16
+//     per instruction) and commits each chunk to that stage's mbarrier;
+//   * the epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM
+//     lanes 32w..32w+31 = tile rows) and applies one of the fused epilogues:
+//       EPI_F32        store (or, split-K, atomically add) FP32 C
+//       EPI_BIAS_SILU  z = acc + b: store z (FP32) and h = silu(z) (BF16)
+//       EPI_DSILU      g = acc * silu'(z_in): store g (BF16), column sums of g
+//                      (the bias gradient) atomically into colsum
+//       EPI_BIAS_F32   store acc + b (FP32)
+// Every mbarrier wait is bounded; on timeout the kernel records an error in the
+// caller's error word, waits (bounded) for its MMAs in flight, skips the
+// epilogue, frees its TMEM and returns.
+//
+// Element-wise kernels of the surrogate: Fourier features (+ their x/y tangents),
+// the MSE loss gradient, Adam, and the FTLE of the network's flow-map Jacobian.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "umma.cuh"
+
+namespace ftle {
+namespace mlp {
+
+constexpr int kTileM = 128;
+constexpr int kStages = 2;
+
+enum { EPI_F32 = 0, EPI_BIAS_SILU = 1, EPI_DSILU = 2, EPI_BIAS_F32 = 3 };
+
+struct Epi {
+  int mode;
+  int ldc;
+  float *c;              // EPI_F32 / EPI_BIAS_F32 output (FP32)
+  const float *bias;     // EPI_BIAS_SILU / EPI_BIAS_F32
+  const float *zin;      // EPI_DSILU pre-activations
+  int ldzin;
+  float *zout;           // EPI_BIAS_SILU pre-activations out (optional)
+  int ldzout;
+  __nv_bfloat16 *hout;   // EPI_BIAS_SILU / EPI_DSILU BF16 output
+  int ldh;
+  float *colsum;         // EPI_DSILU column sums (optional)
+  int accumulate;        // EPI_F32: atomically add into c
+};
+
+// Stage rows [r0, r0+R) x k [k0, k0+kChunkK) of a BF16 matrix with `rows` rows into
+// a K-major smem tile; rows >= `rows` are zero.  TRANS = false: element (r, k) at
+// src[r*ld + k] (16-byte vectors along k); true: at src[k*ld + r] (vectors along r).
+template <bool TRANS>
+__device__ __forceinline__ void stage(unsigned char *tile, const __nv_bfloat16 *__restrict__ src,
+                                      int ld, int rows, int r0, int R, int k0) {
+  if constexpr (!TRANS) {
+    for (int v = threadIdx.x; v < R * (kChunkK / 8); v += blockDim.x) {
+      const int r = v >> 3, c = v & 7;
+      uint4 x = make_uint4(0u, 0u, 0u, 0u);
+      if (r0 + r < rows)
+        x = __ldg(reinterpret_cast<const uint4 *>(src + (long long)(r0 + r) * ld + k0 + 8 * c));
+      *reinterpret_cast<uint4 *>(tile + kmaj_off(r, 8 * c)) = x;
+    }
+  } else {
+    const int groups = R >> 3;
+    for (int v = threadIdx.x; v < kChunkK * groups; v += blockDim.x) {
+      const int k = v / groups, c = v - k * groups;
+      uint4 x = make_uint4(0u, 0u, 0u, 0u);
+      if (r0 + 8 * c < rows)
+        x = __ldg(reinterpret_cast<const uint4 *>(src + (long long)(k0 + k) * ld + r0 + 8 * c));
+      const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+      unsigned char *base = tile + kmaj_off(8 * c, k);  // rows 8c..8c+7 are 16 B apart
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        *reinterpret_cast<unsigned short *>(base + (2 * i) * 16) = (unsigned short)(w[i] & 0xFFFFu);
+        *reinterpret_cast<unsigned short *>(base + (2 * i + 1) * 16) = (unsigned short)(w[i] >> 16);
+      }
+    }
+  }
+}
+
+template <bool A_T, bool B_T>
+__global__ void __launch_bounds__(128, 1)
+    gemm_bf16_kernel(const __nv_bfloat16 *__restrict__ A, int lda,
+                     const __nv_bfloat16 *__restrict__ B, int ldb, int M, int N, int K, int NT,
+                     int k_per_split, Epi epi, int *err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long mbar[kStages];
+  __shared__ uint32_t tmem_slot;
+  __shared__ float colsum_s[256];
+  const int tile_bytes = (kTileM + NT) * kChunkK * 2;
+  const int m0 = blockIdx.x * kTileM;
+  const int n0 = blockIdx.y * NT;
+  const int kbeg = blockIdx.z * k_per_split;
+  const int kend = min(K, kbeg + k_per_split);
+  const int nchunks = kend > kbeg ? (kend - kbeg) / kChunkK : 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t ncols = NT <= 32 ? 32u : (NT <= 64 ? 64u : (NT <= 128 ? 128u : 256u));
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x < kStages) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[threadIdx.x]))
+                 : "memory");
+  }
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) colsum_s[i] = 0.0f;
+  if (threadIdx.x == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = idesc_bf16(kTileM, NT);
+  const uint32_t sbo = kChunkK * 16;
+
+  bool ok = true;
+  for (int c = 0; c < nchunks; ++c) {
+    const int s = c & 1;
+    unsigned char *sA = smem + s * tile_bytes;
+    unsigned char *sB = sA + kTileM * kChunkK * 2;
+    // stage s was last read by the MMAs of chunk c - 2 (its ((c-2)/2)-th commit)
+    if (c >= kStages) ok = mbar_wait(smem_u32(&mbar[s]), (uint32_t)(((c - kStages) >> 1) & 1));
+    if (!__syncthreads_and(ok)) {
+      ok = false;
+      break;
+    }
+    const int k0 = kbeg + c * kChunkK;
+    stage<A_T>(sA, A, lda, M, m0, kTileM, k0);
+    stage<B_T>(sB, B, ldb, N, n0, NT, k0);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < kChunkK / 16; ++j) {
+        const uint64_t ad = smem_desc(smem_u32(sA) + j * 256, 128, sbo);
+        const uint64_t bd = smem_desc(smem_u32(sB) + j * 256, 128, sbo);
+        umma(tmem, ad, bd, idesc, (c > 0 || j > 0) ? 1u : 0u);
+      }
+      umma_commit(smem_u32(&mbar[s]));
+    }
+  }
+  if (ok && nchunks > 0) {
+    // the last commit completes after every earlier MMA of this thread
+    const int c = nchunks - 1;
+    const bool done = mbar_wait(smem_u32(&mbar[c & 1]), (uint32_t)((c >> 1) & 1));
+    ok = __syncthreads_and(done) != 0;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  if (ok && nchunks > 0) {
+    const int row = m0 + 32 * warp + lane;
+    const bool row_ok = row < M;
+    for (int c = 0; c < NT; c += 8) {
+      float v[8];
+      tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, v);
+      const int n = n0 + c;
+      if (n >= N) continue;  // uniform across the CTA
+      if (epi.mode == EPI_F32 || epi.mode == EPI_BIAS_F32) {
+        if (epi.mode == EPI_BIAS_F32) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) v[i] += epi.bias[n + i];
+        }
+        if (row_ok) {
+          float *dst = epi.c + (long long)row * epi.ldc + n;
+          if (epi.accumulate) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) atomicAdd(dst + i, v[i]);
+          } else {
+            reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+            reinterpret_cast<float4 *>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+          }
+        }
+      } else if (epi.mode == EPI_BIAS_SILU) {
+        if (row_ok) {
+          float z[8];
+          uint32_t packed[4];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) z[i] = v[i] + epi.bias[n + i];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 hh = __floats2bfloat162_rn(z[2 * i] * sigmoidf_(z[2 * i]),
+                                                            z[2 * i + 1] * sigmoidf_(z[2 * i + 1]));
+            packed[i] = *reinterpret_cast<const uint32_t *>(&hh);
+          }
+          *reinterpret_cast<uint4 *>(epi.hout + (long long)row * epi.ldh + n) =
+              make_uint4(packed[0], packed[1], packed[2], packed[3]);
+          if (epi.zout) {
+            float *zd = epi.zout + (long long)row * epi.ldzout + n;
+            reinterpret_cast<float4 *>(zd)[0] = make_float4(z[0], z[1], z[2], z[3]);
+            reinterpret_cast<float4 *>(zd)[1] = make_float4(z[4], z[5], z[6], z[7]);
+          }
+        }
+      } else {  // EPI_DSILU
+        float g[8];
+        if (row_ok) {
+          const float *zs = epi.zin + (long long)row * epi.ldzin + n;
+          const float4 za = reinterpret_cast<const float4 *>(zs)[0];
+          const float4 zb = reinterpret_cast<const float4 *>(zs)[1];
+          const float z[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
+          uint32_t packed[4];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const float sg = sigmoidf_(z[i]);
+            g[i] = v[i] * dsilu_from(z[i] * sg, sg);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const __nv_bfloat162 hh = __floats2bfloat162_rn(g[2 * i], g[2 * i + 1]);
+            packed[i] = *reinterpret_cast<const uint32_t *>(&hh);
+            // the bias gradient sums the values the next GEMM consumes
+            g[2 * i] = __low2float(hh);
+            g[2 * i + 1] = __high2float(hh);
+          }
+          *reinterpret_cast<uint4 *>(epi.hout + (long long)row * epi.ldh + n) =
+              make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) g[i] = 0.0f;
+        }
+        if (epi.colsum) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            float s = g[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+            if (lane == 0) atomicAdd(&colsum_s[c + i], s);
+          }
+        }
+      }
+    }
+    if (epi.mode == EPI_DSILU && epi.colsum) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < NT && n0 + i < N; i += blockDim.x)
+        atomicAdd(epi.colsum + n0 + i, colsum_s[i]);
+    }
+  } else if (!ok) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+    // let MMAs still in flight drain (bounded) before the accumulator is freed
+    if (nchunks > 0) {
+      const int c = nchunks - 1;
+      mbar_wait(smem_u32(&mbar[c & 1]), (uint32_t)((c >> 1) & 1));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
+                 : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Element-wise kernels
+// ---------------------------------------------------------------------------
+
+// phase_f = kx_f x + ky_f y + kt_f t + c_f;  features [sin(phase) | cos(phase)] (BF16),
+// optional tangents d/dx, d/dy of the features (BF16).  points: n x 3 FP64 (x, y, t).
+__global__ void features_kernel(const double *__restrict__ pts, long long n,
+                                const float4 *__restrict__ freq, int F,
+                                __nv_bfloat16 *__restrict__ feat, __nv_bfloat16 *__restrict__ tx,
+                                __nv_bfloat16 *__restrict__ ty) {
+  const long long total = n * F;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / F;
+    const int f = (int)(e - p * F);
+    const float4 k = freq[f];
+    // the phase is formed and reduced in FP64 so large coordinates keep precision
+    const double ph = (double)k.x * pts[3 * p] + (double)k.y * pts[3 * p + 1] +
+                      (double)k.z * pts[3 * p + 2] + (double)k.w;
+    const double two_pi = 6.283185307179586;
+    const float r = (float)(ph - two_pi * floor(ph / two_pi));
+    float s, c;
+    sincosf(r, &s, &c);
+    const long long row = p * (2 * F);
+    feat[row + f] = __float2bfloat16_rn(s);
+    feat[row + F + f] = __float2bfloat16_rn(c);
+    if (tx) {
+      tx[row + f] = __float2bfloat16_rn(k.x * c);
+      tx[row + F + f] = __float2bfloat16_rn(-k.x * s);
+    }
+    if (ty) {
+      ty[row + f] = __float2bfloat16_rn(k.y * c);
+      ty[row + F + f] = __float2bfloat16_rn(-k.y * s);
+    }
+  }
+}
+
+// Loss = sum over rows and the `outs` used columns of (y - target)^2 / n;
+// dY = 2 (y - target) / n in BF16 (padded columns zero); the output layer's bias
+// gradient (column sums of the BF16 dY) and the loss are added atomically.
+__global__ void mse_grad_kernel(const float *__restrict__ y, int ldy,
+                                const float *__restrict__ target, int outs, long long n,
+                                float inv_n, __nv_bfloat16 *__restrict__ dy, int lddy,
+                                float *__restrict__ dbias, float *__restrict__ loss) {
+  __shared__ float part[8][5];
+  float acc_loss = 0.0f;
+  float acc_g[4] = {0.f, 0.f, 0.f, 0.f};
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    for (int c = 0; c < lddy; ++c) {
+      float g = 0.0f;
+      if (c < outs) {
+        const float d = y[r * ldy + c] - target[r * outs + c];
+        acc_loss += d * d;
+        g = 2.0f * d * inv_n;
+      }
+      const __nv_bfloat16 gb = __float2bfloat16_rn(g);
+      dy[r * lddy + c] = gb;
+      if (c < outs) acc_g[c] += __bfloat162float(gb);
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    acc_loss += __shfl_xor_sync(0xFFFFFFFFu, acc_loss, o);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc_g[c] += __shfl_xor_sync(0xFFFFFFFFu, acc_g[c], o);
+  }
+  if (lane == 0) {
+    part[warp][0] = acc_loss;
+    for (int c = 0; c < 4; ++c) part[warp][1 + c] = acc_g[c];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float l = 0.f, g[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      l += part[w][0];
+      for (int c = 0; c < 4; ++c) g[c] += part[w][1 + c];
+    }
+    atomicAdd(loss, l * inv_n);
+    for (int c = 0; c < outs; ++c) atomicAdd(dbias + c, g[c]);
+  }
+}
+
+// Adam (decoupled weight decay) on FP32 master parameters; refreshes the BF16
+// copy the GEMMs read and zeroes the gradient for the next step's accumulation.
+__global__ void adam_kernel(float *__restrict__ w, float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, __nv_bfloat16 *__restrict__ wb, long long n,
+                            float lr, float b1, float b2, float eps, float c1, float c2,
+                            float weight_decay) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float mh = mi / c1, vh = vi / c2;
+    const float wi = w[i] - lr * (mh / (sqrtf(vh) + eps) + weight_decay * w[i]);
+    w[i] = wi;
+    wb[i] = __float2bfloat16_rn(wi);
+    g[i] = 0.0f;
+  }
+}
+
+// FTLE of x -> x + s * net(x): F = I + s [dY/dx dY/dy], C = F^T F, lambda_max of the
+// 2x2 symmetric C in closed form, ftle = log(sqrt(lambda)) / |T| (FP64).
+__global__ void jacobian_ftle_kernel(const float *__restrict__ jx, const float *__restrict__ jy,
+                                     int ld, long long n, double scale, double inv_T,
+                                     double *__restrict__ ftle) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double a = 1.0 + scale * (double)jx[i * ld];      // d x_T / d x0
+    const double b = scale * (double)jy[i * ld];            // d x_T / d y0
+    const double c = scale * (double)jx[i * ld + 1];        // d y_T / d x0
+    const double d = 1.0 + scale * (double)jy[i * ld + 1];  // d y_T / d y0
+    const double c11 = a * a + c * c, c12 = a * b + c * d, c22 = b * b + d * d;
+    const double tr = 0.5 * (c11 + c22), df = 0.5 * (c11 - c22);
+    const double lam = tr + sqrt(df * df + c12 * c12);
+    ftle[i] = log(sqrt(lam)) * inv_T;
+  }
+}
+
+// Predicted end positions: out[i] = x0[i] + s * y[i] (FP64, n x 2).
+__global__ void apply_displacement_kernel(const double *__restrict__ pts,
+                                          const float *__restrict__ y, int ldy, long long n,
+                                          double scale, double *__restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    out[2 * i] = pts[3 * i] + scale * (double)y[i * ldy];
+    out[2 * i + 1] = pts[3 * i + 1] + scale * (double)y[i * ldy + 1];
+  }
+}
+
+inline int ew_blocks(long long n) {
+  const long long b = (n + 255) / 256;
+  const long long cap = (long long)kNumSMs * 16;
+  return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+}  // namespace mlp
+}  // namespace ftle
+
+using namespace ftle;
+using namespace ftle::mlp;
+
+namespace {
+
+int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int b_trans, int M,
+                int N, int K, int splits, const Epi &epi, int32_t *error_word, void *stream) {
+  if (!A || !B || !error_word) return fail_invalid("null operand");
+  if (M <= 0 || N <= 0 || K <= 0) return fail_invalid("GEMM sizes must be positive");
+  if (M % 8 || N % 8) return fail_invalid("M and N must be multiples of 8");
+  if (K % kChunkK) return fail_invalid("K must be a multiple of 64");
+  if (lda % 8 || ldb % 8) return fail_invalid("leading dimensions must be multiples of 8");
+  if (reinterpret_cast<uintptr_t>(A) % 16 || reinterpret_cast<uintptr_t>(B) % 16)
+    return fail_invalid("A and B must be 16-byte aligned");
+  if (!a_trans && lda < K) return fail_invalid("lda < K");
+  if (a_trans && lda < M) return fail_invalid("lda < M");
+  if (!b_trans && ldb < K) return fail_invalid("ldb < K");
+  if (b_trans && ldb < N) return fail_invalid("ldb < N");
+  switch (epi.mode) {
+    case EPI_F32:
+    case EPI_BIAS_F32:
+      if (!epi.c || epi.ldc < N || epi.ldc % 4 || reinterpret_cast<uintptr_t>(epi.c) % 16)
+        return fail_invalid("C must be 16-byte aligned with ldc >= N and ldc %% 4 == 0");
+      if (epi.mode == EPI_BIAS_F32 && !epi.bias) return fail_invalid("bias required");
+      break;
+    case EPI_BIAS_SILU:
+      if (!epi.bias || !epi.hout) return fail_invalid("bias and activation output required");
+      if (epi.zout && (epi.ldzout < N || epi.ldzout % 4 ||
+                       reinterpret_cast<uintptr_t>(epi.zout) % 16))
+        return fail_invalid("Z must be 16-byte aligned with ldz >= N and ldz %% 4 == 0");
+      break;
+    case EPI_DSILU:
+      if (!epi.zin || !epi.hout) return fail_invalid("pre-activations and output required");
+      if (epi.ldzin < N || epi.ldzin % 4 || reinterpret_cast<uintptr_t>(epi.zin) % 16)
+        return fail_invalid("Z must be 16-byte aligned with ldz >= N and ldz %% 4 == 0");
+      break;
+    default:
+      return fail_invalid("unknown epilogue %d", epi.mode);
+  }
+  if ((epi.mode == EPI_BIAS_SILU || epi.mode == EPI_DSILU) &&
+      (epi.ldh < N || epi.ldh % 8 || reinterpret_cast<uintptr_t>(epi.hout) % 16))
+    return fail_invalid("BF16 output must be 16-byte aligned with ldh >= N, ldh %% 8 == 0");
+  const int NT = N >= 256 ? 256 : ((N + 15) / 16) * 16;
+  const int kchunks = K / kChunkK;
+  if (splits < 1) splits = 1;
+  if (epi.mode != EPI_F32 && splits > 1) return fail_invalid("split-K needs the FP32 epilogue");
+  if (splits > kchunks) splits = kchunks;
+  const int k_per_split = ((kchunks + splits - 1) / splits) * kChunkK;
+  splits = (K + k_per_split - 1) / k_per_split;
+  Epi e = epi;
+  if (splits > 1) e.accumulate = 1;
+  const size_t smem = (size_t)kStages * (kTileM + NT) * kChunkK * 2;
+  const dim3 grid((M + kTileM - 1) / kTileM, (N + NT - 1) / NT, splits);
+  cudaStream_t st = as_stream(stream);
+  const __nv_bfloat16 *a = static_cast<const __nv_bfloat16 *>(A);
+  const __nv_bfloat16 *b = static_cast<const __nv_bfloat16 *>(B);
+#define GL(AT, BT)                                                                              \
+  do {                                                                                          \
+    cudaFuncSetAttribute(gemm_bf16_kernel<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                         (int)smem);                                                            \
+    gemm_bf16_kernel<AT, BT>                                                                    \
+        <<<grid, 128, smem, st>>>(a, lda, b, ldb, M, N, K, NT, k_per_split, e, error_word);     \
+  } while (0)
+  if (!a_trans && !b_trans)
+    GL(false, false);
+  else if (!a_trans && b_trans)
+    GL(false, true);
+  else if (a_trans && !b_trans)
+    GL(true, false);
+  else
+    GL(true, true);
+#undef GL
+  return check_launch("gemm_bf16_kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+int ftle_mlp_gemm(const void *A, int32_t lda, int32_t a_trans, const void *B, int32_t ldb,
+                  int32_t b_trans, float *C, int32_t ldc, int32_t M, int32_t N, int32_t K,
+                  int32_t splits, int32_t accumulate, int32_t *error_word, void *stream) {
+  Epi e{};
+  e.mode = EPI_F32;
+  e.c = C;
+  e.ldc = ldc;
+  e.accumulate = accumulate;
+  return gemm_launch(A, lda, a_trans, B, ldb, b_trans, M, N, K, splits, e, error_word, stream);
+}
+
+int ftle_mlp_linear(const void *X, int32_t ldx, const void *W, int32_t ldw, const float *bias,
+                    int32_t M, int32_t N, int32_t K, int32_t activation, float *Z, int32_t ldz,
+                    void *H, int32_t ldh, int32_t *error_word, void *stream) {
+  Epi e{};
+  if (activation) {
+    e.mode = EPI_BIAS_SILU;
+    e.bias = bias;
+    e.zout = Z;
+    e.ldzout = ldz;
+    e.hout = static_cast<__nv_bfloat16 *>(H);
+    e.ldh = ldh;
+  } else {
+    e.mode = EPI_BIAS_F32;
+    e.bias = bias;
+    e.c = Z;
+    e.ldc = ldz;
+  }
+  return gemm_launch(X, ldx, 0, W, ldw, 0, M, N, K, 1, e, error_word, stream);
+}
+
+int ftle_mlp_gemm_dsilu(const void *A, int32_t lda, int32_t a_trans, const void *B, int32_t ldb,
+                        int32_t b_trans, int32_t M, int32_t N, int32_t K, const float *Zin,
+                        int32_t ldz, void *G, int32_t ldg, float *colsum, int32_t *error_word,
+                        void *stream) {
+  Epi e{};
+  e.mode = EPI_DSILU;
+  e.zin = Zin;
+  e.ldzin = ldz;
+  e.hout = static_cast<__nv_bfloat16 *>(G);
+  e.ldh = ldg;
+  e.colsum = colsum;
+  return gemm_launch(A, lda, a_trans, B, ldb, b_trans, M, N, K, 1, e, error_word, stream);
+}
+
+int ftle_mlp_features(const double *points, int64_t n, const float *freq, int32_t num_freq,
+                      void *features, void *tangent_x, void *tangent_y, void *stream) {
+  if (n < 0 || num_freq <= 0) return fail_invalid("bad sizes");
+  if (n == 0) return FTLE_OK;
+  if (!points || !freq || !features) return fail_invalid("null pointer");
+  if (reinterpret_cast<uintptr_t>(freq) % 16) return fail_invalid("freq must be 16-byte aligned");
+  features_kernel<<<ew_blocks(n * num_freq), 256, 0, as_stream(stream)>>>(
+      points, n, reinterpret_cast<const float4 *>(freq), num_freq,
+      static_cast<__nv_bfloat16 *>(features), static_cast<__nv_bfloat16 *>(tangent_x),
+      static_cast<__nv_bfloat16 *>(tangent_y));
+  return check_launch("features_kernel");
+}
+
+int ftle_mlp_mse_grad(const float *y, int32_t ldy, const float *target, int32_t outs, int64_t n,
+                      void *dy, int32_t lddy, float *dbias, float *loss, void *stream) {
+  if (n <= 0 || outs <= 0 || outs > 4 || lddy < outs || ldy < outs)
+    return fail_invalid("bad sizes");
+  if (!y || !target || !dy || !dbias || !loss) return fail_invalid("null pointer");
+  mse_grad_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(
+      y, ldy, target, outs, n, 1.0f / (float)n, static_cast<__nv_bfloat16 *>(dy), lddy, dbias,
+      loss);
+  return check_launch("mse_grad_kernel");
+}
+
+int ftle_mlp_adam(float *w, float *g, float *m, float *v, void *w_bf16, int64_t n, float lr,
+                  float beta1, float beta2, float eps, int32_t step, float weight_decay,
+                  void *stream) {
+  if (n <= 0 || step < 1) return fail_invalid("bad sizes");
+  if (!w || !g || !m || !v || !w_bf16) return fail_invalid("null pointer");
+  const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+  adam_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(
+      w, g, m, v, static_cast<__nv_bfloat16 *>(w_bf16), n, lr, beta1, beta2, eps, c1, c2,
+      weight_decay);
+  return check_launch("adam_kernel");
+}
+
+int ftle_mlp_jacobian_ftle(const float *jx, const float *jy, int32_t ld, int64_t n, double scale,
+                           double T, double *ftle, void *stream) {
+  if (n < 0 || ld < 2 || T == 0.0) return fail_invalid("bad sizes");
+  if (n == 0) return FTLE_OK;
+  if (!jx || !jy || !ftle) return fail_invalid("null pointer");
+  jacobian_ftle_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(jx, jy, ld, n, scale,
+                                                                     1.0 / fabs(T), ftle);
+  return check_launch("jacobian_ftle_kernel");
+}
+
+int ftle_mlp_apply_displacement(const double *points, const float *y, int32_t ldy, int64_t n,
+                                double scale, double *out, void *stream) {
+  if (n < 0 || ldy < 2) return fail_invalid("bad sizes");
+  if (n == 0) return FTLE_OK;
+  if (!points || !y || !out) return fail_invalid("null pointer");
+  apply_displacement_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(points, y, ldy, n, scale,
+                                                                          out);
+  return check_launch("apply_displacement_kernel");
+}
+
+}  // extern "C"

@@ -64,6 +64,16 @@ def seeds_2d(centroids: np.ndarray, delta: float) -> np.ndarray:
     return np.concatenate((c - ex, c + ex, c + ey, c - ey), axis=0)
 
 
+def seeds_2d_device(centroids, delta: float):
+    """seeds_2d for a (N, 2) float64 device tensor of centroids (stays on the device)."""
+    import torch
+
+    c = centroids
+    ex = torch.tensor([delta, 0.0], dtype=torch.float64, device=c.device)
+    ey = torch.tensor([0.0, delta], dtype=torch.float64, device=c.device)
+    return torch.cat((c - ex, c + ex, c + ey, c - ey), dim=0).contiguous()
+
+
 def seeds_3d(centroids: np.ndarray, delta: float) -> np.ndarray:
     """Role-blocked (6N, 3) neighbours [L; R; T; B; F; Bk] around (N, 3) centroids."""
     c = np.asarray(centroids, dtype=np.float64)
