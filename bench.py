@@ -419,6 +419,9 @@ def run_ours(args):
                 "frac": achieved / peak, "traffic": traffic,
                 "peak_source": peak_src,
                 "algorithmic_bytes_per_particle_step": bytes_per_ps,
+                "algorithmic_bytes_per_launch": bytes_per_ps * K * N * (
+                    chunk if chunk else w["num_steps"]),
+                "traffic_note": "DRAM bytes per launch from ncu at this workload",
                 "kernel": "window_mixed_kernel" if elem == 2 else "window_f64_kernel",
                 "kernel_ms": kernel_ms}
 
