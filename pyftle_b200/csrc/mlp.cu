@@ -1,15 +1,18 @@
 // mlp.cu -- BF16 tensor-core (tcgen05 / TMEM) kernels of the flow-map surrogate MLP.
 //
 // GEMM: C[M x N] (+)= A[M x K] * B[N x K]^T, BF16 operands, FP32 accumulation in
-// tensor memory.  One CTA (4 warps) owns a 128 x NT tile (NT <= 256) of C:
-//   * operands are staged in shared memory in the no-swizzle K-major "core
-//     matrix" layout (8 rows x 16 bytes per core matrix, K chunks 128 B apart,
-//     8-row groups KC*16 B apart), two stages deep so the loads of chunk c+1
-//     overlap the MMAs of chunk c; the loader reads A/B either row-major or
-//     transposed, so every product of training (X W^T, dZ W, dZ^T X) and of the
-//     Jacobian tangents runs through this one kernel; rows past M (or N) load as 0;
+// tensor memory.  One CTA (4 warps) owns a 128 x NT tile (NT <= 128) of C:
+//   * operands are staged in shared memory as no-swizzle core matrices (8 x 16 B):
+//     an operand stored row-major (K contiguous) as K-major tiles, an operand stored
+//     transposed (its M/N index contiguous) as MN-major tiles with the descriptor's
+//     major bit set, so both are copied as 16-byte vectors with no transposition;
+//     every product of training (X W^T, dZ W, dZ^T X) and of the Jacobian tangents
+//     runs through this one kernel; rows past M (or N) are zero-filled;
+//   * loads are cp.async 16-byte copies in a 3-stage ring, so chunks c+1 and c+2
+//     are in flight while the tensor core works on chunk c;
 //   * one elected thread issues tcgen05.mma (kind::f16, M = 128, N = NT, K = 16
-//     per instruction) and commits each chunk to that stage's mbarrier;
+//     per instruction) and commits each chunk to that stage's mbarrier, which
+//     frees the stage for the copies of chunk c + 3;
 //   * the epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM
 //     lanes 32w..32w+31 = tile rows) and applies one of the fused epilogues:
 //       EPI_F32        store (or, split-K, atomically add) FP32 C
@@ -18,8 +21,8 @@
 //                      (the bias gradient) atomically into colsum
 //       EPI_BIAS_F32   store acc + b (FP32)
 // Every mbarrier wait is bounded; on timeout the kernel records an error in the
-// caller's error word, waits (bounded) for its MMAs in flight, skips the
-// epilogue, frees its TMEM and returns.
+// caller's error word, waits (bounded) for its copies and MMAs in flight, skips
+// the epilogue, frees its TMEM and returns.
 //
 // Element-wise kernels of the surrogate: Fourier features (+ their x/y tangents),
 // the MSE loss gradient, Adam, and the FTLE of the network's flow-map Jacobian.
@@ -32,7 +35,8 @@ namespace ftle {
 namespace mlp {
 
 constexpr int kTileM = 128;
-constexpr int kStages = 2;
+constexpr int kStages = 3;
+constexpr int kMaxNT = 128;
 
 enum { EPI_F32 = 0, EPI_BIAS_SILU = 1, EPI_DSILU = 2, EPI_BIAS_F32 = 3 };
 
@@ -51,34 +55,48 @@ struct Epi {
   int accumulate;        // EPI_F32: atomically add into c
 };
 
-// Stage rows [r0, r0+R) x k [k0, k0+kChunkK) of a BF16 matrix with `rows` rows into
-// a K-major smem tile; rows >= `rows` are zero.  TRANS = false: element (r, k) at
-// src[r*ld + k] (16-byte vectors along k); true: at src[k*ld + r] (vectors along r).
+// Byte offset of element (r, k) of an R x kChunkK MN-major tile (no swizzle): the
+// core matrix of rows 8i..8i+7 and K 8j..8j+7 holds 8 K-rows of 16 B (8 consecutive
+// r each); K groups 128 B apart (leading byte offset), row groups kChunkK*16 B apart
+// (stride byte offset) -- the same descriptor strides as the K-major tiles.
+__device__ __forceinline__ uint32_t mn_off(int r, int k) {
+  return (uint32_t)((r >> 3) * (kChunkK * 16) + (k >> 3) * 128 + (k & 7) * 16 + (r & 7) * 2);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
+  // src-size 0 zero-fills the 16 bytes without reading
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Issue the copies of rows [r0, r0+R) x k [k0, k0+kChunkK) of a BF16 matrix with
+// `rows` rows into a smem tile; rows >= `rows` are zero-filled.  TRANS = false:
+// element (r, k) at src[r*ld + k] -> K-major tile; true: at src[k*ld + r] -> MN-major.
 template <bool TRANS>
-__device__ __forceinline__ void stage(unsigned char *tile, const __nv_bfloat16 *__restrict__ src,
-                                      int ld, int rows, int r0, int R, int k0) {
+__device__ __forceinline__ void stage_async(uint32_t tile, const __nv_bfloat16 *__restrict__ src,
+                                            int ld, int rows, int r0, int R, int k0) {
   if constexpr (!TRANS) {
     for (int v = threadIdx.x; v < R * (kChunkK / 8); v += blockDim.x) {
       const int r = v >> 3, c = v & 7;
-      uint4 x = make_uint4(0u, 0u, 0u, 0u);
-      if (r0 + r < rows)
-        x = __ldg(reinterpret_cast<const uint4 *>(src + (long long)(r0 + r) * ld + k0 + 8 * c));
-      *reinterpret_cast<uint4 *>(tile + kmaj_off(r, 8 * c)) = x;
+      const bool ok = r0 + r < rows;
+      const __nv_bfloat16 *p = ok ? src + (long long)(r0 + r) * ld + k0 + 8 * c : src;
+      cp_async16(tile + kmaj_off(r, 8 * c), p, ok);
     }
   } else {
     const int groups = R >> 3;
     for (int v = threadIdx.x; v < kChunkK * groups; v += blockDim.x) {
       const int k = v / groups, c = v - k * groups;
-      uint4 x = make_uint4(0u, 0u, 0u, 0u);
-      if (r0 + 8 * c < rows)
-        x = __ldg(reinterpret_cast<const uint4 *>(src + (long long)(k0 + k) * ld + r0 + 8 * c));
-      const uint32_t w[4] = {x.x, x.y, x.z, x.w};
-      unsigned char *base = tile + kmaj_off(8 * c, k);  // rows 8c..8c+7 are 16 B apart
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        *reinterpret_cast<unsigned short *>(base + (2 * i) * 16) = (unsigned short)(w[i] & 0xFFFFu);
-        *reinterpret_cast<unsigned short *>(base + (2 * i + 1) * 16) = (unsigned short)(w[i] >> 16);
-      }
+      const bool ok = r0 + 8 * c < rows;
+      const __nv_bfloat16 *p = ok ? src + (long long)(k0 + k) * ld + r0 + 8 * c : src;
+      cp_async16(tile + mn_off(8 * c, k), p, ok);
     }
   }
 }
@@ -91,7 +109,7 @@ __global__ void __launch_bounds__(128, 1)
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) unsigned long long mbar[kStages];
   __shared__ uint32_t tmem_slot;
-  __shared__ float colsum_s[256];
+  __shared__ float colsum_s[kMaxNT];
   const int tile_bytes = (kTileM + NT) * kChunkK * 2;
   const int m0 = blockIdx.x * kTileM;
   const int n0 = blockIdx.y * NT;
@@ -99,62 +117,68 @@ __global__ void __launch_bounds__(128, 1)
   const int kend = min(K, kbeg + k_per_split);
   const int nchunks = kend > kbeg ? (kend - kbeg) / kChunkK : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t ncols = NT <= 32 ? 32u : (NT <= 64 ? 64u : (NT <= 128 ? 128u : 256u));
+  const uint32_t ncols = NT <= 32 ? 32u : (NT <= 64 ? 64u : 128u);
+  const uint32_t smem0 = smem_u32(smem);
 
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(&tmem_slot)),
-                 "r"(ncols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  if (threadIdx.x < kStages) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[threadIdx.x]))
-                 : "memory");
-  }
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) colsum_s[i] = 0.0f;
+  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), ncols);
+  if (threadIdx.x < kStages) mbar_init(smem_u32(&mbar[threadIdx.x]), 1);
+  for (int i = threadIdx.x; i < kMaxNT; i += blockDim.x) colsum_s[i] = 0.0f;
   if (threadIdx.x == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  fence_before_sync();
   __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  fence_after_sync();
   const uint32_t tmem = tmem_slot;
-  const uint32_t idesc = idesc_bf16(kTileM, NT);
+  // A and B are K-major unless stored transposed (MN-major: bits 15 / 16)
+  const uint32_t idesc =
+      idesc_bf16(kTileM, NT) | (A_T ? (1u << 15) : 0u) | (B_T ? (1u << 16) : 0u);
   const uint32_t sbo = kChunkK * 16;
 
+  auto load_chunk = [&](int c) {
+    const uint32_t sA = smem0 + (c % kStages) * tile_bytes;
+    const uint32_t sB = sA + kTileM * kChunkK * 2;
+    const int k0 = kbeg + c * kChunkK;
+    stage_async<A_T>(sA, A, lda, M, m0, kTileM, k0);
+    stage_async<B_T>(sB, B, ldb, N, n0, NT, k0);
+  };
+  for (int c = 0; c < kStages - 1; ++c) {
+    if (c < nchunks) load_chunk(c);
+    cp_async_commit();
+  }
   bool ok = true;
   for (int c = 0; c < nchunks; ++c) {
-    const int s = c & 1;
-    unsigned char *sA = smem + s * tile_bytes;
-    unsigned char *sB = sA + kTileM * kChunkK * 2;
-    // stage s was last read by the MMAs of chunk c - 2 (its ((c-2)/2)-th commit)
-    if (c >= kStages) ok = mbar_wait(smem_u32(&mbar[s]), (uint32_t)(((c - kStages) >> 1) & 1));
+    cp_async_wait<kStages - 2>();  // this thread's copies of chunk c landed
+    fence_proxy_async_smem();       // ... and are visible to the tensor core
     if (!__syncthreads_and(ok)) {
       ok = false;
       break;
     }
-    const int k0 = kbeg + c * kChunkK;
-    stage<A_T>(sA, A, lda, M, m0, kTileM, k0);
-    stage<B_T>(sB, B, ldb, N, n0, NT, k0);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
     if (threadIdx.x == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      fence_after_sync();
+      const uint32_t sA = smem0 + (c % kStages) * tile_bytes;
+      const uint32_t sB = sA + kTileM * kChunkK * 2;
 #pragma unroll
       for (int j = 0; j < kChunkK / 16; ++j) {
-        const uint64_t ad = smem_desc(smem_u32(sA) + j * 256, 128, sbo);
-        const uint64_t bd = smem_desc(smem_u32(sB) + j * 256, 128, sbo);
-        umma(tmem, ad, bd, idesc, (c > 0 || j > 0) ? 1u : 0u);
+        umma(tmem, smem_desc(sA + j * 256, 128, sbo), smem_desc(sB + j * 256, 128, sbo), idesc,
+             (c > 0 || j > 0) ? 1u : 0u);
       }
-      umma_commit(smem_u32(&mbar[s]));
+      umma_commit(smem_u32(&mbar[c % kStages]));
     }
+    // chunk c + kStages - 1 refills the stage chunk c - 1 used, once its MMAs are done
+    const int nc = c + kStages - 1;
+    if (nc < nchunks) {
+      if (c >= 1)
+        ok = mbar_wait(smem_u32(&mbar[(c - 1) % kStages]), (uint32_t)(((c - 1) / kStages) & 1));
+      if (ok) load_chunk(nc);
+    }
+    cp_async_commit();
   }
   if (ok && nchunks > 0) {
     // the last commit completes after every earlier MMA of this thread
     const int c = nchunks - 1;
-    const bool done = mbar_wait(smem_u32(&mbar[c & 1]), (uint32_t)((c >> 1) & 1));
+    const bool done = mbar_wait(smem_u32(&mbar[c % kStages]), (uint32_t)((c / kStages) & 1));
     ok = __syncthreads_and(done) != 0;
   }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  fence_after_sync();
 
   if (ok && nchunks > 0) {
     const int row = m0 + 32 * warp + lane;
@@ -247,14 +271,13 @@ __global__ void __launch_bounds__(128, 1)
     // let MMAs still in flight drain (bounded) before the accumulator is freed
     if (nchunks > 0) {
       const int c = nchunks - 1;
-      mbar_wait(smem_u32(&mbar[c & 1]), (uint32_t)((c >> 1) & 1));
+      mbar_wait(smem_u32(&mbar[c % kStages]), (uint32_t)((c / kStages) & 1));
     }
   }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
+  fence_before_sync();
   __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
-                 : "memory");
+  if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
 // ---------------------------------------------------------------------------
@@ -442,7 +465,7 @@ int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int
   if ((epi.mode == EPI_BIAS_SILU || epi.mode == EPI_DSILU) &&
       (epi.ldh < N || epi.ldh % 8 || reinterpret_cast<uintptr_t>(epi.hout) % 16))
     return fail_invalid("BF16 output must be 16-byte aligned with ldh >= N, ldh %% 8 == 0");
-  const int NT = N >= 256 ? 256 : ((N + 15) / 16) * 16;
+  const int NT = N >= kMaxNT ? kMaxNT : ((N + 15) / 16) * 16;
   const int kchunks = K / kChunkK;
   if (splits < 1) splits = 1;
   if (epi.mode != EPI_F32 && splits > 1) return fail_invalid("split-K needs the FP32 epilogue");
