@@ -49,7 +49,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["abc", "batched", "gyre", "abc256"], default="abc",
+    p.add_argument("--workload", choices=["abc", "batched", "gyre", "abc256", "surrogate"],
+                   default="abc",
                    help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
                         "turbulence windows in one persistent launch")
     p.add_argument("--precision", choices=["fx15", "fp16", "bf16", "fp64"], default="fx15")
@@ -70,6 +71,14 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-clocks", action="store_true")
+    p.add_argument("--train-samples", type=int, default=50_000_000,
+                   help="surrogate: RK4 trajectories in the training set")
+    p.add_argument("--train-steps", type=int, default=4000, help="surrogate: Adam steps")
+    p.add_argument("--sur-windows", type=int, default=200, help="surrogate: sliding windows")
+    p.add_argument("--sur-seeds", type=int, default=1024, help="surrogate: seeds per axis")
+    p.add_argument("--kmax", type=float, default=128.0,
+                   help="surrogate: largest wavenumber of the turbulence field")
+    p.add_argument("--tol", type=float, default=1e-3, help="surrogate: judge tolerance")
     return p.parse_args()
 
 
@@ -718,6 +727,136 @@ def run_abc256(args):
     return 0
 
 
+def run_surrogate(args):
+    """Learned flow-map surrogate over sliding windows of the 2D turbulence field.
+
+    Field as the batched workload (1024^2 periodic, 400 snapshots, dt = 0.05,
+    u_rms = --urms, wavenumbers 4..--kmax).  Windows of fixed T = 5 (RK4 h = 0.025,
+    200 steps) start at t0 = i*dt.  The MLP (64 Fourier features of (x0, y0, t0),
+    4 x 256 SiLU, BF16) is trained by the engine's tensor-core kernels on
+    --train-samples FP64 RK4 trajectories with start times from the window starts.
+    Each window's field on a --sur-seeds^2 seed grid (delta 5e-4) is computed twice:
+    the surrogate form (fused network + Jacobian FTLE, RK4 on 1% of the seeds of
+    every 32 x 32 region as the judge, RK4 re-advection of every region whose error
+    exceeds --tol) and the method without it (FX15 mixed RK4 for every seed).
+    """
+    import torch
+
+    from pyftle_b200 import SnapshotSeries, flows
+    from pyftle_b200.interpolate import GridSpec
+    from pyftle_b200.surrogate import SurrogateFTLE, TrainConfig, fit_flow_map
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, S, dt, h, T = 1024, 400, 0.05, 0.025, 5.0
+    L = 2 * math.pi
+    turb = flows.FourierTurbulence2D(seed=7, num_modes=256, kmin=4, kmax=args.kmax,
+                                     urms=args.urms)
+    snaps = turb.snapshots_device(n, np.arange(S) * dt)
+    ax = flows.periodic_axis(n)
+    grid = GridSpec(shape=(n, n), origin=(0.0, 0.0), spacing=(ax[1], ax[1]), periodic=True)
+    s64 = SnapshotSeries(grid, snaps, precision="fp64")
+    sfx = SnapshotSeries(grid, snaps, precision="fx15")
+    del snaps
+    starts = np.arange(args.sur_windows) * dt
+    net, fit = fit_flow_map(s64, T=T, h=h, snapshot_dt=dt, t0_values=starts,
+                            num_samples=args.train_samples,
+                            cfg=TrainConfig(steps=args.train_steps, batch=65536, lr=2e-3))
+    m = args.sur_seeds
+    sp = L / m
+    sur = SurrogateFTLE(net, sfx, nx=m, ny=m, origin=(0.5 * sp, 0.5 * sp), spacing=(sp, sp),
+                        T=T, h=h, snapshot_dt=dt, delta=5e-4, tile=32, tol=args.tol)
+    for t0 in starts[:args.warmup]:
+        sur.field(float(t0))
+        sur.reference_field(float(t0))
+    torch.cuda.synchronize()
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    tols = sorted({args.tol, 1e-2, 3e-2, 1e-1, 3e-1})
+    t_sur = t_rk = t_eval = 0.0
+    judged_err, raw_err, acc = [], [], []
+    readv_windows = 0
+    sweep = {t: {"accepted": [], "err_num": 0.0, "rejected_frac": []} for t in tols}
+    ref_norm2 = 0.0
+    for t0 in starts:
+        t0 = float(t0)
+        e = [ev() for _ in range(4)]
+        e[0].record()
+        f, rep = sur.field(t0)
+        e[1].record()
+        ref = sur.reference_field(t0)
+        e[2].record()
+        fs, sref, rerr = sur.evaluate(t0)
+        e[3].record()
+        torch.cuda.synchronize()
+        t_sur += e[0].elapsed_time(e[1])
+        t_rk += e[1].elapsed_time(e[2])
+        t_eval += e[2].elapsed_time(e[3])
+        rn = float(torch.linalg.vector_norm(ref))
+        ref_norm2 += rn * rn
+        judged_err.append(float(torch.linalg.vector_norm(f - ref)) / rn)
+        raw_err.append(float(torch.linalg.vector_norm(fs - ref)) / rn)
+        acc.append(rep.accepted_fraction)
+        readv_windows += int(rep.rejected > 0)
+        d = fs - ref
+        d[sur.sample_idx] = 0.0
+        for tl in tols:
+            ok = (rerr <= tl)[sur.region_of]
+            sweep[tl]["err_num"] += float(torch.sum((d * ok) ** 2))
+            sweep[tl]["accepted"].append(float((rerr <= tl).double().mean()))
+    W = len(starts)
+    rk_fields = W / (t_rk / 1e3)
+    sur_fields = W / (t_sur / 1e3)
+    eval_ms = t_eval / W
+    rk_ms = t_rk / W
+    sweep_out = []
+    for tl in tols:
+        a = float(np.mean(sweep[tl]["accepted"]))
+        est_ms = eval_ms + (1.0 - a) * rk_ms  # surrogate + judge, then re-advection
+        sweep_out.append({"tol": tl, "accepted_regions": a,
+                          "ftle_rel_err_l2": math.sqrt(sweep[tl]["err_num"] / ref_norm2),
+                          "est_fields_per_s": 1e3 / est_ms,
+                          "est_speedup_vs_rk4": rk_ms / est_ms})
+    # the surrogate form against FP64 plain RK4 on two windows
+    err64 = []
+    for t0 in (float(starts[0]), float(starts[W // 2])):
+        f, _ = sur.field(t0)
+        from pyftle_b200 import flows as fl
+        from pyftle_b200.window import run_window
+        pos = fl.seeds_2d_device(sur.centroids, 5e-4)
+        f64 = run_window(s64, pos, integrator="rk4", time_mode="blend", h=h,
+                         num_steps=int(round(T / h)), t0=t0, snapshot_dt=dt)
+        err64.append(float(torch.linalg.vector_norm(f - f64) / torch.linalg.vector_norm(f64)))
+    sp_steps = 4 * m * m * int(round(T / h))
+    line = {
+        "metric": "FTLE fields/s, surrogate form (1% RK4 judge, RK4 re-advection) vs RK4",
+        "value": sur_fields, "unit": "fields/s", "n_gpus": 1, "steps": W,
+        "warmup": args.warmup, "ms_per_step": t_sur / W, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": f"2D turbulence 1024^2 periodic, 400 snapshots dt=0.05, "
+                               f"k in [4,{args.kmax:g}], u_rms={args.urms}; {W} sliding "
+                               f"windows T=5 (RK4 h=0.025) on {m}^2 seeds, delta 5e-4; "
+                               f"judge tol {args.tol:g} on 1% of each 32x32 region",
+                   "network": "64 Fourier features of (x0,y0,t0) -> 4x256 SiLU -> 2, BF16",
+                   "training": fit},
+        "rk4_fields_per_s": rk_fields,
+        "rk4_particle_steps_per_s": sp_steps * rk_fields,
+        "speedup_vs_rk4": sur_fields / rk_fields,
+        "accepted_regions_mean": float(np.mean(acc)),
+        "ftle_rel_err_l2_judged_vs_rk4": {"max": max(judged_err), "mean": float(np.mean(judged_err))},
+        "ftle_rel_err_l2_raw_surrogate_vs_rk4": {"max": max(raw_err), "mean": float(np.mean(raw_err))},
+        "ftle_rel_err_l2_judged_vs_fp64": err64,
+        "surrogate_and_judge_ms_per_field": eval_ms, "rk4_ms_per_field": rk_ms,
+        "tolerance_sweep": sweep_out,
+        # per window: the fused network kernel, the judge's RK4 window, and one RK4
+        # window over the rejected regions when there are any
+        "gpu_launches": 2 * W + readv_windows,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.workload == "abc256" and args.impl != "reference":
@@ -728,6 +867,8 @@ def main():
         return run_batched(args)
     if args.workload == "gyre":
         return run_gyre(args)
+    if args.workload == "surrogate":
+        return run_surrogate(args)
     return run_ours(args)
 
 

@@ -424,6 +424,35 @@ def train(net: FlowMapMLP, points: torch.Tensor, displacement: torch.Tensor,
     return log
 
 
+def fit_flow_map(series64, *, T: float, h: float, snapshot_dt: float, t0_values,
+                 num_samples: int, length: float = 2.0 * math.pi,
+                 freq: Optional[np.ndarray] = None, cfg: TrainConfig = TrainConfig(),
+                 seed: int = 0) -> Tuple[FlowMapMLP, Dict[str, float]]:
+    """Train a FlowMapMLP on ``num_samples`` RK4 trajectories of the series: seeds
+    uniform on the periodic box [0, length)^2, start times drawn from ``t0_values``.
+    Returns the network and timings (seconds) of data generation and training."""
+    import time
+
+    dev = require_cuda()
+    g = torch.Generator(device=dev).manual_seed(seed)
+    pts = torch.rand(num_samples, 3, generator=g, device=dev, dtype=torch.float64)
+    pts[:, :2] *= length
+    t0v = torch.as_tensor(np.asarray(t0_values, dtype=np.float64), device=dev)
+    pts[:, 2] = t0v[torch.randint(0, t0v.numel(), (num_samples,), generator=g, device=dev)]
+    torch.cuda.synchronize()
+    a = time.perf_counter()
+    disp = rk4_displacements(series64, pts, T=T, h=h, snapshot_dt=snapshot_dt)
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    net = FlowMapMLP(freq if freq is not None else fourier_frequencies(32, length=length),
+                     out_scale=float(disp.abs().max()), seed=seed)
+    log = train(net, pts, disp, cfg)
+    torch.cuda.synchronize()
+    c = time.perf_counter()
+    return net, {"data_s": b - a, "train_s": c - b, "final_loss": log[-1][1],
+                 "samples": num_samples, "steps": cfg.steps, "batch": cfg.batch}
+
+
 # ---------------------------------------------------------------------------------------
 # surrogate FTLE with the RK4 judge
 # ---------------------------------------------------------------------------------------
@@ -499,14 +528,16 @@ class SurrogateFTLE:
                           num_steps=self.steps, t0=t0, snapshot_dt=self.snapshot_dt,
                           chunk_steps=self.rk4_chunk_steps)
 
-    def field(self, t0: float, judge: bool = True) -> Tuple[torch.Tensor, Optional[JudgeReport]]:
+    def surrogate_field(self, t0: float) -> torch.Tensor:
+        """The network's FTLE for every seed (no judge)."""
         if self.net.supports_fused:
-            f = self.net.ftle_fused(self.centroids, t0, self.T)
-        else:
-            self.points[:, 2] = t0
-            f = self.net.ftle(self.points, self.T)
-        if not judge:
-            return f, None
+            return self.net.ftle_fused(self.centroids, t0, self.T)
+        self.points[:, 2] = t0
+        return self.net.ftle(self.points, self.T)
+
+    def evaluate(self, t0: float) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """(surrogate field, RK4 FTLE of the sampled seeds, error of every region)."""
+        f = self.surrogate_field(t0)
         ref = self._rk4_ftle(self.sample_idx, t0)
         err = (f[self.sample_idx] - ref) ** 2
         R = self.num_regions
@@ -515,17 +546,44 @@ class SurrogateFTLE:
         cnt = torch.zeros(R, dtype=torch.float64, device=f.device).index_add_(
             0, self.sample_region, torch.ones_like(err))
         scale = torch.sqrt(torch.mean(ref * ref)).clamp_min(1e-300)
-        region_err = torch.sqrt(num / cnt.clamp_min(1)) / scale
+        return f, ref, torch.sqrt(num / cnt.clamp_min(1)) / scale
+
+    def field(self, t0: float, judge: bool = True,
+              tol: Optional[float] = None) -> Tuple[torch.Tensor, Optional[JudgeReport]]:
+        """FTLE field of the window starting at t0: surrogate where the judge accepts,
+        RK4 at the sampled seeds and in every rejected region."""
+        if not judge:
+            return self.surrogate_field(t0), None
+        tol = self.tol if tol is None else float(tol)
+        f, ref, region_err = self.evaluate(t0)
         f[self.sample_idx] = ref
-        bad = torch.nonzero(region_err > self.tol).squeeze(1).cpu().numpy()
+        bad = torch.nonzero(region_err > tol).squeeze(1).cpu().numpy()
         readv = 0
-        if bad.size:
+        if bad.size == self.num_regions:
+            f = self.reference_field(t0)
+            readv = self.nx * self.ny
+        elif bad.size:
             seeds = torch.cat([self.region_seeds[int(r)] for r in bad])
             f[seeds] = self._rk4_ftle(seeds, t0)
             readv = int(seeds.numel())
-        rep = JudgeReport(regions=R, rejected=int(bad.size), sampled=int(self.sample_idx.numel()),
-                          readvected_seeds=readv, region_errors=region_err.cpu().numpy())
+        rep = JudgeReport(regions=self.num_regions, rejected=int(bad.size),
+                          sampled=int(self.sample_idx.numel()), readvected_seeds=readv,
+                          region_errors=region_err.cpu().numpy())
         return f, rep
+
+    def run(self, starts: Sequence[float], writer=None):
+        """Sliding windows starting at each of ``starts``.  Returns the fields (host
+        arrays) and the judge reports, or writes ``ftle_<t0>`` files with ``writer``."""
+        fields, reports = [], []
+        for t0 in starts:
+            f, rep = self.field(float(t0))
+            reports.append(rep)
+            arr = f.cpu().numpy()
+            if writer is not None:
+                writer.write(f"ftle_{float(t0):06f}", arr, self.centroids.cpu().numpy())
+            else:
+                fields.append(arr)
+        return (None if writer is not None else fields), reports
 
     def reference_field(self, t0: float) -> torch.Tensor:
         """RK4 FTLE of every seed (the method without the surrogate)."""
