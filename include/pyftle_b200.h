@@ -277,6 +277,17 @@ int ftle_mlp_jacobian_ftle(const float *jx, const float *jy, int32_t ld, int64_t
 /* out (n x 2 FP64) = points[:, :2] + scale * y[:, :2]. */
 int ftle_mlp_apply_displacement(const double *points, const float *y, int32_t ldy, int64_t n,
                                 double scale, double *out, void *stream);
+/* 3D forms: points n x 4 FP64 (x, y, z, t); freq num_freq rows of 8 FP32
+ * (kx, ky, kz, kt, phase, 0, 0, 0); tangents d/dx, d/dy, d/dz (each may be NULL);
+ * the FTLE from the three tangents (columns 0..2) with lambda_max of the 3x3
+ * Cauchy-Green tensor by Jacobi rotations; end positions n x 3. */
+int ftle_mlp_features3(const double *points, int64_t n, const float *freq, int32_t num_freq,
+                       void *features, void *tangent_x, void *tangent_y, void *tangent_z,
+                       void *stream);
+int ftle_mlp_jacobian_ftle3(const float *jx, const float *jy, const float *jz, int32_t ld,
+                            int64_t n, double scale, double T, double *ftle, void *stream);
+int ftle_mlp_apply_displacement3(const double *points, const float *y, int32_t ldy, int64_t n,
+                                 double scale, double *out, void *stream);
 
 /* Fused surrogate inference for the fixed shape 32 frequencies (64 features) ->
  * 4 x 256 SiLU -> 2 outputs: one persistent launch evaluates the network and its

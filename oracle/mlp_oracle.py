@@ -50,17 +50,20 @@ def dsilu(z):
 
 
 def features(points: np.ndarray, freq: np.ndarray, tangents: bool = False):
-    """points (n, 3) = (x, y, t); freq (F, 4) = (kx, ky, kt, phase)."""
+    """2D: points (n, 3) = (x, y, t), freq (F, 4) = (kx, ky, kt, phase);
+    3D: points (n, 4) = (x, y, z, t), freq (F, 8) = (kx, ky, kz, kt, phase, 0, 0, 0).
+    Returns the features, and with ``tangents`` their derivatives along each
+    spatial axis (tx, ty(, tz))."""
     p = np.asarray(points, dtype=np.float64)
     k = np.asarray(freq, dtype=np.float32).astype(np.float64)
-    ph = p @ k[:, :3].T + k[:, 3]
+    d = p.shape[1] - 1
+    ph = p @ k[:, :d + 1].T + k[:, d + 1]
     s, c = np.sin(ph), np.cos(ph)
     feat = np.concatenate([s, c], axis=1)
     if not tangents:
         return feat
-    tx = np.concatenate([k[:, 0] * c, -k[:, 0] * s], axis=1)
-    ty = np.concatenate([k[:, 1] * c, -k[:, 1] * s], axis=1)
-    return feat, tx, ty
+    return (feat,) + tuple(np.concatenate([k[:, a] * c, -k[:, a] * s], axis=1)
+                           for a in range(d))
 
 
 def forward(feat: np.ndarray, weights: Sequence[np.ndarray], biases: Sequence[np.ndarray],
@@ -100,16 +103,36 @@ def loss_and_grads(feat, weights, biases, target, outs: int, bf16_points: bool =
     return loss, gW, gb, Y
 
 
-def jacobian(feat, tx, ty, weights, biases, bf16_points: bool = True):
-    """Forward-mode tangents dY/dx, dY/dy through the network."""
+def jacobian_n(feat, tangents, weights, biases, bf16_points: bool = True):
+    """Forward-mode tangents dY/dx_a through the network, one per seed tangent."""
     r = bf16 if bf16_points else _id
     fw = forward(feat, weights, biases, bf16_points)
     out = []
-    for t in (tx, ty):
+    for t in tangents:
         t = r(t)
         for l, W in enumerate(weights):
             t = t @ r(W).T
             if l < len(weights) - 1:
                 t = r(t * dsilu(fw["Z"][l]))
         out.append(t)
-    return fw["Y"], out[0], out[1]
+    return fw["Y"], out
+
+
+def jacobian(feat, tx, ty, weights, biases, bf16_points: bool = True):
+    """2D form of jacobian_n: (Y, dY/dx, dY/dy)."""
+    y, (jx, jy) = jacobian_n(feat, (tx, ty), weights, biases, bf16_points)
+    return y, jx, jy
+
+
+def ftle_from_tangents(J, scale: float, T: float) -> np.ndarray:
+    """FTLE of x -> x + scale * y(x) from the tangents J[a] = dY/dx_a (n, >= dim):
+    F = I + scale * [dY_r/dx_a], C = F^T F, largest eigenvalue in float64."""
+    d = len(J)
+    n = J[0].shape[0]
+    F = np.empty((n, d, d))
+    for a in range(d):
+        F[:, :, a] = scale * J[a][:, :d]
+    F += np.eye(d)
+    C = np.einsum("nra,nrb->nab", F, F)
+    lam = np.linalg.eigvalsh(C)[:, -1]
+    return np.log(np.sqrt(lam)) / abs(T)

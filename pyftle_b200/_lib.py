@@ -105,6 +105,12 @@ SIGNATURES = {
                                               _c_dp]),
     "ftle_mlp_apply_displacement": (ctypes.c_int, [_c_dp, _c_dp, _i32, _i64, _f64, _c_dp,
                                                    _c_dp]),
+    "ftle_mlp_features3": (ctypes.c_int, [_c_dp, _i64, _c_dp, _i32, _c_dp, _c_dp, _c_dp, _c_dp,
+                                          _c_dp]),
+    "ftle_mlp_jacobian_ftle3": (ctypes.c_int, [_c_dp, _c_dp, _c_dp, _i32, _i64, _f64, _f64,
+                                               _c_dp, _c_dp]),
+    "ftle_mlp_apply_displacement3": (ctypes.c_int, [_c_dp, _c_dp, _i32, _i64, _f64, _c_dp,
+                                                    _c_dp]),
     "ftle_surrogate_packed_bytes": (ctypes.c_int64, []),
     "ftle_surrogate_pack": (ctypes.c_int, [_c_dp, _c_dp, _c_dp, _c_dp, _c_dp, _c_dp, _c_dp]),
     "ftle_surrogate_ftle": (ctypes.c_int, [_c_dp, _i64, _f64, _c_dp, _c_dp, _c_dp, _f64, _f64,

@@ -77,4 +77,45 @@ __device__ __forceinline__ long long node3(const GridK &g, int i, int j, int k) 
   return ((long long)j * g.n[0] + i) * g.n[2] + k;
 }
 
+// Largest eigenvalue of a symmetric 3x3 matrix by cyclic Jacobi rotations (FP64);
+// the mixed-precision window epilogue and the 3D surrogate's FTLE use it.
+static __device__ __noinline__ double lmax3_sym(double a00, double a01, double a02, double a11,
+                                                double a12, double a22) {
+  double a[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
+  for (int sweep = 0; sweep < 32; ++sweep) {
+    const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
+    const double diag = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
+    if (off == 0.0 || off <= 1e-300 || off < 1e-18 * diag) break;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+#pragma unroll
+      for (int q = p + 1; q < 3; ++q) {
+        const double apq = a[p][q];
+        if (apq == 0.0) continue;
+        const double app = a[p][p], aqq = a[q][q];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0);
+        const double s = t * c;
+        a[p][p] = app - t * apq;
+        a[q][q] = aqq + t * apq;
+        a[p][q] = 0.0;
+        a[q][p] = 0.0;
+        const int r = 3 - p - q;
+        const double arp = a[r][p], arq = a[r][q];
+        const double nrp = c * arp - s * arq;
+        const double nrq = s * arp + c * arq;
+        a[r][p] = nrp;
+        a[p][r] = nrp;
+        a[r][q] = nrq;
+        a[q][r] = nrq;
+      }
+    }
+  }
+  double mx = a[0][0];
+  if (a[1][1] > mx) mx = a[1][1];
+  if (a[2][2] > mx) mx = a[2][2];
+  return mx;
+}
+
 }  // namespace ftle

@@ -454,44 +454,6 @@ __device__ __forceinline__ double lmax2(double F00, double F01, double F10, doub
   return (l2 > l1) ? l2 : l1;
 }
 
-__device__ __noinline__ double lmax3_sym(double a00, double a01, double a02, double a11,
-                                         double a12, double a22) {
-  double a[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
-  for (int sweep = 0; sweep < 32; ++sweep) {
-    const double off = fabs(a[0][1]) + fabs(a[0][2]) + fabs(a[1][2]);
-    const double diag = fabs(a[0][0]) + fabs(a[1][1]) + fabs(a[2][2]);
-    if (off == 0.0 || off <= 1e-300 || off < 1e-18 * diag) break;
-#pragma unroll
-    for (int p = 0; p < 2; ++p) {
-#pragma unroll
-      for (int q = p + 1; q < 3; ++q) {
-        const double apq = a[p][q];
-        if (apq == 0.0) continue;
-        const double app = a[p][p], aqq = a[q][q];
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-        const double c = 1.0 / sqrt(t * t + 1.0);
-        const double s = t * c;
-        a[p][p] = app - t * apq;
-        a[q][q] = aqq + t * apq;
-        a[p][q] = 0.0;
-        a[q][p] = 0.0;
-        const int r = 3 - p - q;
-        const double arp = a[r][p], arq = a[r][q];
-        const double nrp = c * arp - s * arq;
-        const double nrq = s * arp + c * arq;
-        a[r][p] = nrp;
-        a[p][r] = nrp;
-        a[r][q] = nrq;
-        a[q][r] = nrq;
-      }
-    }
-  }
-  double mx = a[0][0];
-  if (a[1][1] > mx) mx = a[1][1];
-  if (a[2][2] > mx) mx = a[2][2];
-  return mx;
-}
 
 // Off-cell neighbour work items of one warp (structure of arrays, per warp).
 template <int DIM>

@@ -414,6 +414,74 @@ __global__ void apply_displacement_kernel(const double *__restrict__ pts,
   }
 }
 
+// 3D features: points n x 4 FP64 (x, y, z, t); freq rows of 8 FP32
+// (kx, ky, kz, kt, phase, 0, 0, 0); tangents d/dx, d/dy, d/dz (each may be null).
+__global__ void features3_kernel(const double *__restrict__ pts, long long n,
+                                 const float4 *__restrict__ freq, int F,
+                                 __nv_bfloat16 *__restrict__ feat, __nv_bfloat16 *__restrict__ tx,
+                                 __nv_bfloat16 *__restrict__ ty, __nv_bfloat16 *__restrict__ tz) {
+  const long long total = n * F;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / F;
+    const int f = (int)(e - p * F);
+    const float4 k = freq[2 * f];
+    const float ph0 = freq[2 * f + 1].x;
+    const double ph = (double)k.x * pts[4 * p] + (double)k.y * pts[4 * p + 1] +
+                      (double)k.z * pts[4 * p + 2] + (double)k.w * pts[4 * p + 3] + (double)ph0;
+    const double two_pi = 6.283185307179586;
+    const float r = (float)(ph - two_pi * floor(ph / two_pi));
+    float sn, cs;
+    sincosf(r, &sn, &cs);
+    const long long row = p * (2 * F);
+    feat[row + f] = __float2bfloat16_rn(sn);
+    feat[row + F + f] = __float2bfloat16_rn(cs);
+    __nv_bfloat16 *t[3] = {tx, ty, tz};
+    const float kk[3] = {k.x, k.y, k.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (t[a]) {
+        t[a][row + f] = __float2bfloat16_rn(kk[a] * cs);
+        t[a][row + F + f] = __float2bfloat16_rn(-kk[a] * sn);
+      }
+    }
+  }
+}
+
+// 3D FTLE of x -> x + s * net(x): F[r][j] = delta_rj + s * dY_r/dx_j (tangent j's
+// column r), C = F^T F, lambda_max by Jacobi rotations, ftle = log(sqrt(lambda))/|T|.
+__global__ void jacobian_ftle3_kernel(const float *__restrict__ jx, const float *__restrict__ jy,
+                                      const float *__restrict__ jz, int ld, long long n,
+                                      double scale, double inv_T, double *__restrict__ ftle) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float *J[3] = {jx + i * ld, jy + i * ld, jz + i * ld};
+    double F[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) F[r][j] = (r == j ? 1.0 : 0.0) + scale * (double)J[j][r];
+    double C[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) C[a][b] = F[0][a] * F[0][b] + F[1][a] * F[1][b] + F[2][a] * F[2][b];
+    const double lam = lmax3_sym(C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+    ftle[i] = log(sqrt(lam)) * inv_T;
+  }
+}
+
+// 3D predicted end positions: out[i] = x0[i] + s * y[i] (FP64, n x 3; points n x 4).
+__global__ void apply_displacement3_kernel(const double *__restrict__ pts,
+                                           const float *__restrict__ y, int ldy, long long n,
+                                           double scale, double *__restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[3 * i + a] = pts[4 * i + a] + scale * (double)y[i * ldy + a];
+  }
+}
+
 inline int ew_blocks(long long n) {
   const long long b = (n + 255) / 256;
   const long long cap = (long long)kNumSMs * 16;
@@ -601,6 +669,40 @@ int ftle_mlp_apply_displacement(const double *points, const float *y, int32_t ld
   apply_displacement_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(points, y, ldy, n, scale,
                                                                           out);
   return check_launch("apply_displacement_kernel");
+}
+
+int ftle_mlp_features3(const double *points, int64_t n, const float *freq, int32_t num_freq,
+                       void *features, void *tangent_x, void *tangent_y, void *tangent_z,
+                       void *stream) {
+  if (n < 0 || num_freq <= 0) return fail_invalid("bad sizes");
+  if (n == 0) return FTLE_OK;
+  if (!points || !freq || !features) return fail_invalid("null pointer");
+  if (reinterpret_cast<uintptr_t>(freq) % 16) return fail_invalid("freq must be 16-byte aligned");
+  features3_kernel<<<ew_blocks(n * num_freq), 256, 0, as_stream(stream)>>>(
+      points, n, reinterpret_cast<const float4 *>(freq), num_freq,
+      static_cast<__nv_bfloat16 *>(features), static_cast<__nv_bfloat16 *>(tangent_x),
+      static_cast<__nv_bfloat16 *>(tangent_y), static_cast<__nv_bfloat16 *>(tangent_z));
+  return check_launch("features3_kernel");
+}
+
+int ftle_mlp_jacobian_ftle3(const float *jx, const float *jy, const float *jz, int32_t ld,
+                            int64_t n, double scale, double T, double *ftle, void *stream) {
+  if (n < 0 || ld < 3 || T == 0.0) return fail_invalid("bad sizes");
+  if (n == 0) return FTLE_OK;
+  if (!jx || !jy || !jz || !ftle) return fail_invalid("null pointer");
+  jacobian_ftle3_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(jx, jy, jz, ld, n, scale,
+                                                                      1.0 / fabs(T), ftle);
+  return check_launch("jacobian_ftle3_kernel");
+}
+
+int ftle_mlp_apply_displacement3(const double *points, const float *y, int32_t ldy, int64_t n,
+                                 double scale, double *out, void *stream) {
+  if (n < 0 || ldy < 3) return fail_invalid("bad sizes");
+  if (n == 0) return FTLE_OK;
+  if (!points || !y || !out) return fail_invalid("null pointer");
+  apply_displacement3_kernel<<<ew_blocks(n), 256, 0, as_stream(stream)>>>(points, y, ldy, n,
+                                                                           scale, out);
+  return check_launch("apply_displacement3_kernel");
 }
 
 }  // extern "C"

@@ -74,6 +74,18 @@ def seeds_2d_device(centroids, delta: float):
     return torch.cat((c - ex, c + ex, c + ey, c - ey), dim=0).contiguous()
 
 
+def seeds_3d_device(centroids, delta: float):
+    """seeds_3d for a (N, 3) float64 device tensor of centroids (stays on the device)."""
+    import torch
+
+    c = centroids
+    e = [torch.zeros(3, dtype=torch.float64, device=c.device) for _ in range(3)]
+    for a in range(3):
+        e[a][a] = delta
+    return torch.cat((c - e[0], c + e[0], c + e[1], c - e[1], c + e[2], c - e[2]),
+                     dim=0).contiguous()
+
+
 def seeds_3d(centroids: np.ndarray, delta: float) -> np.ndarray:
     """Role-blocked (6N, 3) neighbours [L; R; T; B; F; Bk] around (N, 3) centroids."""
     c = np.asarray(centroids, dtype=np.float64)

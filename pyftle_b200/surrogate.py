@@ -31,25 +31,29 @@ from pyftle_b200._device import ptr, require_cuda, stream_ptr
 
 def fourier_frequencies(num: int = 32, *, length: float = 2.0 * math.pi,
                         space_sigma: float = 6.0, time_sigma: float = 0.3,
-                        seed: int = 0) -> np.ndarray:
-    """(num, 4) float32 rows (kx, ky, kt, phase): integer wavenumbers on the periodic
-    box [0, length)^2 (the features stay periodic), Gaussian time frequencies.
-    The first rows are the pure spatial unit modes, so the lowest harmonics are
-    always present."""
+                        seed: int = 0, dim: int = 2) -> np.ndarray:
+    """Frequency rows: 2D (num, 4) float32 (kx, ky, kt, phase); 3D (num, 8) float32
+    (kx, ky, kz, kt, phase, 0, 0, 0).  Integer wavenumbers on the periodic box
+    [0, length)^dim (the features stay periodic), Gaussian time frequencies.  The
+    first rows are pure spatial unit modes, so the lowest harmonics are always present."""
+    if dim not in (2, 3):
+        raise ValueError("dim must be 2 or 3")
     rng = np.random.default_rng(seed)
     k0 = 2.0 * math.pi / length
-    rows = [(1, 0), (0, 1), (1, 1), (1, -1)]
-    out = np.zeros((num, 4), dtype=np.float32)
+    rows = ([(1, 0), (0, 1), (1, 1), (1, -1)] if dim == 2 else
+            [(1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (0, 1, 1), (1, 0, 1)])
+    out = np.zeros((num, 4 if dim == 2 else 8), dtype=np.float32)
     for i in range(num):
         if i < len(rows):
-            kx, ky, kt = rows[i][0], rows[i][1], 0.0
+            k, kt = rows[i], 0.0
         else:
             while True:
-                kx, ky = np.round(rng.normal(0.0, space_sigma, 2)).astype(int)
-                if kx or ky:
+                k = np.round(rng.normal(0.0, space_sigma, dim)).astype(int)
+                if np.any(k):
                     break
             kt = rng.normal(0.0, time_sigma)
-        out[i] = (kx * k0, ky * k0, kt, 0.0)
+        out[i, :dim] = np.asarray(k, dtype=np.float64) * k0
+        out[i, dim] = kt
     return out
 
 
@@ -63,18 +67,22 @@ class _Layer:
 
 
 class FlowMapMLP:
-    """features(x, y, t0) -> [hidden x depth, SiLU] -> displacement / out_scale."""
+    """features(x0, t0) -> [hidden x depth, SiLU] -> displacement / out_scale, in 2D
+    (freq rows of 4: points (x, y, t0)) or 3D (freq rows of 8: points (x, y, z, t0))."""
 
     OUT_PAD = 64
 
-    def __init__(self, freq: np.ndarray, *, hidden: int = 256, depth: int = 4, outs: int = 2,
-                 out_scale: float = 1.0, seed: int = 0, device=None):
+    def __init__(self, freq: np.ndarray, *, hidden: int = 256, depth: int = 4,
+                 outs: Optional[int] = None, out_scale: float = 1.0, seed: int = 0,
+                 device=None):
         self.device = device or require_cuda()
         freq = np.ascontiguousarray(freq, dtype=np.float32)
-        if freq.ndim != 2 or freq.shape[1] != 4 or (2 * freq.shape[0]) % 64:
-            raise ValueError("freq must be (F, 4) with 2F a multiple of 64")
-        if hidden % 64 or hidden > 256:
-            raise ValueError("hidden width must be a multiple of 64, at most 256")
+        if freq.ndim != 2 or freq.shape[1] not in (4, 8) or (2 * freq.shape[0]) % 64:
+            raise ValueError("freq must be (F, 4) (2D) or (F, 8) (3D) with 2F a multiple of 64")
+        self.dim = 2 if freq.shape[1] == 4 else 3
+        outs = self.dim if outs is None else int(outs)
+        if hidden % 64 or hidden > 1024:
+            raise ValueError("hidden width must be a multiple of 64, at most 1024")
         self.freq_np = freq
         self.freq = torch.from_numpy(freq).to(self.device)
         self.in_features = 2 * freq.shape[0]
@@ -160,12 +168,15 @@ class FlowMapMLP:
         ws = {"feat": torch.empty(rows, F, dtype=bf, device=dev),
               "tx": torch.empty(rows, F, dtype=bf, device=dev),
               "ty": torch.empty(rows, F, dtype=bf, device=dev),
+              "tz": torch.empty(rows, F, dtype=bf, device=dev) if self.dim == 3 else None,
               "Y": torch.empty(rows, self.OUT_PAD, dtype=f32, device=dev),
               "dY": torch.empty(rows, self.OUT_PAD, dtype=bf, device=dev),
               "Ga": torch.empty(rows, H, dtype=bf, device=dev),
               "Gb": torch.empty(rows, H, dtype=bf, device=dev),
               "Jx": torch.empty(rows, self.OUT_PAD, dtype=f32, device=dev),
               "Jy": torch.empty(rows, self.OUT_PAD, dtype=f32, device=dev),
+              "Jz": (torch.empty(rows, self.OUT_PAD, dtype=f32, device=dev)
+                     if self.dim == 3 else None),
               "loss": torch.zeros(1, dtype=f32, device=dev)}
         for l in range(self.depth):
             ws[f"Z{l}"] = torch.empty(rows, H, dtype=f32, device=dev)
@@ -176,9 +187,13 @@ class FlowMapMLP:
     # ---- passes ----------------------------------------------------------------------
     def _features(self, points: torch.Tensor, n: int, tangents: bool):
         ws = self._workspace(n)
-        _lib.call("ftle_mlp_features", ptr(points), n, ptr(self.freq), self.freq.shape[0],
-                  ptr(ws["feat"]), ptr(ws["tx"] if tangents else None),
-                  ptr(ws["ty"] if tangents else None), stream_ptr())
+        t = (lambda k: ws[k] if tangents else None)
+        if self.dim == 2:
+            _lib.call("ftle_mlp_features", ptr(points), n, ptr(self.freq), self.freq.shape[0],
+                      ptr(ws["feat"]), ptr(t("tx")), ptr(t("ty")), stream_ptr())
+        else:
+            _lib.call("ftle_mlp_features3", ptr(points), n, ptr(self.freq), self.freq.shape[0],
+                      ptr(ws["feat"]), ptr(t("tx")), ptr(t("ty")), ptr(t("tz")), stream_ptr())
         return ws
 
     def _forward(self, ws, n: int):
@@ -213,41 +228,45 @@ class FlowMapMLP:
                           self.OUT_PAD, n, L.out_pad, L.fan_in, 1, 0, ptr(self.err), s)
 
     def predict(self, points: torch.Tensor, jacobian: bool = False):
-        """points (n, 3) float64 CUDA (x, y, t0).  Returns the network output Y
+        """points (n, dim+1) float64 CUDA (x0, t0).  Returns the network output Y
         (n, OUT_PAD) FP32 views (displacement / out_scale in columns :outs), and with
-        ``jacobian`` the tangents dY/dx, dY/dy (views into the workspace; valid until
-        the next call)."""
+        ``jacobian`` the tangents dY/dx (, dY/dy, dY/dz) (views into the workspace;
+        valid until the next call)."""
         n = self._check_points(points)
         ws = self._features(points, n, jacobian)
         self._forward(ws, n)
         if not jacobian:
             return ws["Y"][:n]
-        self._tangent(ws, n, "tx", "Jx")
-        self._tangent(ws, n, "ty", "Jy")
-        return ws["Y"][:n], ws["Jx"][:n], ws["Jy"][:n]
+        keys = (("tx", "Jx"), ("ty", "Jy"), ("tz", "Jz"))[:self.dim]
+        for seed, out in keys:
+            self._tangent(ws, n, seed, out)
+        return (ws["Y"][:n],) + tuple(ws[o][:n] for _, o in keys)
 
     def ftle(self, points: torch.Tensor, T: float, out: Optional[torch.Tensor] = None,
              chunk: int = 1 << 20) -> torch.Tensor:
-        """FTLE (float64) of the surrogate flow map at points (n, 3), in chunks."""
+        """FTLE (float64) of the surrogate flow map at points (n, dim+1), in chunks."""
         n = self._check_points(points)
         if out is None:
             out = torch.empty(n, dtype=torch.float64, device=points.device)
         for i in range(0, n, chunk):
             j = min(n, i + chunk)
-            _, jx, jy = self.predict(points[i:j], jacobian=True)
-            _lib.call("ftle_mlp_jacobian_ftle", ptr(jx), ptr(jy), self.OUT_PAD, j - i,
-                      self.out_scale, float(T), ptr(out[i:j]), stream_ptr())
+            _, *J = self.predict(points[i:j], jacobian=True)
+            name = "ftle_mlp_jacobian_ftle" if self.dim == 2 else "ftle_mlp_jacobian_ftle3"
+            _lib.call(name, *(ptr(x) for x in J), self.OUT_PAD, j - i, self.out_scale,
+                      float(T), ptr(out[i:j]), stream_ptr())
         return out
 
     def end_positions(self, points: torch.Tensor, chunk: int = 1 << 20) -> torch.Tensor:
-        """x0 + predicted displacement, (n, 2) float64."""
+        """x0 + predicted displacement, (n, dim) float64."""
         n = self._check_points(points)
-        out = torch.empty(n, 2, dtype=torch.float64, device=points.device)
+        out = torch.empty(n, self.dim, dtype=torch.float64, device=points.device)
+        name = ("ftle_mlp_apply_displacement" if self.dim == 2
+                else "ftle_mlp_apply_displacement3")
         for i in range(0, n, chunk):
             j = min(n, i + chunk)
             y = self.predict(points[i:j])
-            _lib.call("ftle_mlp_apply_displacement", ptr(points[i:j]), ptr(y), self.OUT_PAD,
-                      j - i, self.out_scale, ptr(out[i:j]), stream_ptr())
+            _lib.call(name, ptr(points[i:j]), ptr(y), self.OUT_PAD, j - i, self.out_scale,
+                      ptr(out[i:j]), stream_ptr())
         return out
 
     def loss_and_grads(self, points: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
@@ -297,8 +316,8 @@ class FlowMapMLP:
     @property
     def supports_fused(self) -> bool:
         """The fused kernel's fixed shape: 32 frequencies, 4 x 256 hidden, 2 outputs."""
-        return (self.in_features == 64 and self.hidden == 256 and self.depth == 4
-                and self.outs == 2)
+        return (self.dim == 2 and self.in_features == 64 and self.hidden == 256
+                and self.depth == 4 and self.outs == 2)
 
     def _fused_params(self):
         if getattr(self, "_fused_key", None) == (self.step, id(self.w)) and self._fused is not None:
@@ -338,9 +357,10 @@ class FlowMapMLP:
             raise RuntimeError("a tensor-core wait timed out in an MLP kernel")
 
     def _check_points(self, points: torch.Tensor) -> int:
+        d = self.dim + 1
         if points.dtype != torch.float64 or not points.is_cuda or not points.is_contiguous() \
-                or points.ndim != 2 or points.shape[1] != 3:
-            raise ValueError("points must be a contiguous (n, 3) float64 CUDA tensor")
+                or points.ndim != 2 or points.shape[1] != d:
+            raise ValueError(f"points must be a contiguous (n, {d}) float64 CUDA tensor")
         n = points.shape[0]
         if n % 8:
             raise ValueError("the number of points must be a multiple of 8")
@@ -353,24 +373,27 @@ class FlowMapMLP:
 
 def rk4_displacements(series, points: torch.Tensor, *, T: float, h: float,
                       snapshot_dt: float, chunk: int = 1 << 22) -> torch.Tensor:
-    """Displacement (n, 2) float64 of each (x, y, t0) point over T by RK4 through the
-    series (time-blended, the engine's window kernel; points with equal t0 share a
-    launch).  The series' precision picks the kernel (FP64 plain or mixed)."""
+    """Displacement (n, dim) float64 of each (x0, t0) point (n, dim+1) over T by RK4
+    through an FP64 series (time-blended; the plain window kernel advects every point
+    independently; points with equal t0 share a launch)."""
     from pyftle_b200.window import run_window
 
+    if series.storage != _lib.F64:
+        raise ValueError("training trajectories come from an FP64 series")
+    dim = series.grid.dim
     steps = int(round(T / h))
     if abs(steps * h - T) > 1e-9 * max(1.0, T):
         raise ValueError("T must be a whole number of steps h")
-    t0s = points[:, 2]
+    t0s = points[:, dim]
     uniq = torch.unique(t0s).cpu().numpy()
-    out = torch.empty(points.shape[0], 2, dtype=torch.float64, device=points.device)
+    out = torch.empty(points.shape[0], dim, dtype=torch.float64, device=points.device)
     for t0 in uniq:
         idx = torch.nonzero(t0s == float(t0)).squeeze(1)
         for i in range(0, idx.numel(), chunk):
             sel = idx[i:i + chunk]
             m = sel.numel()
-            pad = (-m) % 4
-            p = points[sel, :2]
+            pad = (-m) % (2 * dim)
+            p = points[sel, :dim]
             if pad:
                 p = torch.cat([p, p[:pad]])
             p = p.contiguous()
@@ -426,31 +449,36 @@ def train(net: FlowMapMLP, points: torch.Tensor, displacement: torch.Tensor,
 
 def fit_flow_map(series64, *, T: float, h: float, snapshot_dt: float, t0_values,
                  num_samples: int, length: float = 2.0 * math.pi,
-                 freq: Optional[np.ndarray] = None, cfg: TrainConfig = TrainConfig(),
+                 freq: Optional[np.ndarray] = None, hidden: int = 256, depth: int = 4,
+                 cfg: TrainConfig = TrainConfig(),
                  seed: int = 0) -> Tuple[FlowMapMLP, Dict[str, float]]:
-    """Train a FlowMapMLP on ``num_samples`` RK4 trajectories of the series: seeds
-    uniform on the periodic box [0, length)^2, start times drawn from ``t0_values``.
+    """Train a FlowMapMLP on ``num_samples`` RK4 trajectories of the FP64 series: seeds
+    uniform on the periodic box [0, length)^dim, start times drawn from ``t0_values``.
     Returns the network and timings (seconds) of data generation and training."""
     import time
 
     dev = require_cuda()
+    dim = series64.grid.dim
     g = torch.Generator(device=dev).manual_seed(seed)
-    pts = torch.rand(num_samples, 3, generator=g, device=dev, dtype=torch.float64)
-    pts[:, :2] *= length
+    pts = torch.rand(num_samples, dim + 1, generator=g, device=dev, dtype=torch.float64)
+    pts[:, :dim] *= length
     t0v = torch.as_tensor(np.asarray(t0_values, dtype=np.float64), device=dev)
-    pts[:, 2] = t0v[torch.randint(0, t0v.numel(), (num_samples,), generator=g, device=dev)]
+    pts[:, dim] = t0v[torch.randint(0, t0v.numel(), (num_samples,), generator=g, device=dev)]
     torch.cuda.synchronize()
     a = time.perf_counter()
     disp = rk4_displacements(series64, pts, T=T, h=h, snapshot_dt=snapshot_dt)
     torch.cuda.synchronize()
     b = time.perf_counter()
-    net = FlowMapMLP(freq if freq is not None else fourier_frequencies(32, length=length),
-                     out_scale=float(disp.abs().max()), seed=seed)
+    if freq is None:
+        freq = fourier_frequencies(32, length=length, dim=dim)
+    net = FlowMapMLP(freq, hidden=hidden, depth=depth, out_scale=float(disp.abs().max()),
+                     seed=seed)
     log = train(net, pts, disp, cfg)
     torch.cuda.synchronize()
     c = time.perf_counter()
     return net, {"data_s": b - a, "train_s": c - b, "final_loss": log[-1][1],
-                 "samples": num_samples, "steps": cfg.steps, "batch": cfg.batch}
+                 "samples": num_samples, "steps": cfg.steps, "batch": cfg.batch,
+                 "hidden": hidden, "depth": depth}
 
 
 # ---------------------------------------------------------------------------------------
@@ -480,30 +508,39 @@ class SurrogateFTLE:
     field-level relative L2 error restricted to the region).
     """
 
-    def __init__(self, net: FlowMapMLP, series, *, nx: int, ny: int, origin=(0.0, 0.0),
-                 spacing=(1.0, 1.0), T: float, h: float, snapshot_dt: float,
-                 delta: float = 5e-4, tile: int = 32, sample_fraction: float = 0.01,
-                 tol: float = 1e-3, rk4_chunk_steps: Optional[int] = None, seed: int = 0):
+    def __init__(self, net: FlowMapMLP, series, *, nx: int, ny: int, nz: Optional[int] = None,
+                 origin=(0.0, 0.0, 0.0), spacing=(1.0, 1.0, 1.0), T: float, h: float,
+                 snapshot_dt: float, delta: float = 5e-4, tile: int = 32,
+                 sample_fraction: float = 0.01, tol: float = 1e-3,
+                 rk4_chunk_steps: Optional[int] = None, seed: int = 0):
         self.net, self.series = net, series
-        self.nx, self.ny, self.T, self.h = nx, ny, float(T), float(h)
+        self.dim = 2 if nz is None else 3
+        if net.dim != self.dim or series.grid.dim != self.dim:
+            raise ValueError("network, series and seed grid must have the same dimension")
+        self.nx, self.ny, self.nz = nx, ny, (nz or 1)
+        self.T, self.h = float(T), float(h)
         self.steps = int(round(T / h))
         self.snapshot_dt, self.delta, self.tol = float(snapshot_dt), float(delta), float(tol)
         self.rk4_chunk_steps = rk4_chunk_steps
         dev = net.device
-        xs = origin[0] + spacing[0] * np.arange(nx)
-        ys = origin[1] + spacing[1] * np.arange(ny)
-        X, Y = np.meshgrid(xs, ys)  # seed (i, j) at j*nx + i
-        self.centroids = torch.from_numpy(np.column_stack((X.ravel(), Y.ravel()))).to(dev)
-        n = nx * ny
+        axes = [origin[a] + spacing[a] * np.arange(m)
+                for a, m in enumerate((nx, ny, nz)[:self.dim])]
+        # seeds in the reference's meshgrid-"xy" order: 2D j*nx + i, 3D (j*nx + i)*nz + k
+        grids = np.meshgrid(*axes)
+        self.centroids = torch.from_numpy(np.column_stack([g.ravel() for g in grids])).to(dev)
+        n = self.centroids.shape[0]
         if n % 8:
-            raise ValueError("nx * ny must be a multiple of 8")
-        self.points = torch.empty(n, 3, dtype=torch.float64, device=dev)
-        self.points[:, :2] = self.centroids
-        # regions: tile x tile blocks of seeds; region id of every seed
-        tx, ty = (nx + tile - 1) // tile, (ny + tile - 1) // tile
-        I, J = np.meshgrid(np.arange(nx) // tile, np.arange(ny) // tile)
-        region = (J * tx + I).ravel()
-        self.num_regions = tx * ty
+            raise ValueError("the number of seeds must be a multiple of 8")
+        self.points = torch.empty(n, self.dim + 1, dtype=torch.float64, device=dev)
+        self.points[:, :self.dim] = self.centroids
+        # regions: tile^dim blocks of seeds; region id of every seed
+        counts_ax = [(m + tile - 1) // tile for m in (nx, ny, nz)[:self.dim]]
+        idx = np.meshgrid(*[np.arange(m) // tile for m in (nx, ny, nz)[:self.dim]])
+        if self.dim == 2:
+            region = (idx[1] * counts_ax[0] + idx[0]).ravel()
+        else:
+            region = ((idx[1] * counts_ax[0] + idx[0]) * counts_ax[2] + idx[2]).ravel()
+        self.num_regions = int(np.prod(counts_ax))
         self.region_of = torch.from_numpy(region).to(dev)
         order = np.argsort(region, kind="stable")
         counts = np.bincount(region, minlength=self.num_regions)
@@ -523,7 +560,8 @@ class SurrogateFTLE:
         from pyftle_b200.window import run_window
 
         c = self.centroids[seeds]
-        pos = flows.seeds_2d_device(c, self.delta)
+        pos = (flows.seeds_2d_device(c, self.delta) if self.dim == 2
+               else flows.seeds_3d_device(c, self.delta))
         return run_window(self.series, pos, integrator="rk4", time_mode="blend", h=self.h,
                           num_steps=self.steps, t0=t0, snapshot_dt=self.snapshot_dt,
                           chunk_steps=self.rk4_chunk_steps)
@@ -532,7 +570,7 @@ class SurrogateFTLE:
         """The network's FTLE for every seed (no judge)."""
         if self.net.supports_fused:
             return self.net.ftle_fused(self.centroids, t0, self.T)
-        self.points[:, 2] = t0
+        self.points[:, self.dim] = t0
         return self.net.ftle(self.points, self.T)
 
     def evaluate(self, t0: float) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
@@ -561,7 +599,7 @@ class SurrogateFTLE:
         readv = 0
         if bad.size == self.num_regions:
             f = self.reference_field(t0)
-            readv = self.nx * self.ny
+            readv = self.centroids.shape[0]
         elif bad.size:
             seeds = torch.cat([self.region_seeds[int(r)] for r in bad])
             f[seeds] = self._rk4_ftle(seeds, t0)
@@ -587,5 +625,5 @@ class SurrogateFTLE:
 
     def reference_field(self, t0: float) -> torch.Tensor:
         """RK4 FTLE of every seed (the method without the surrogate)."""
-        all_idx = torch.arange(self.nx * self.ny, device=self.centroids.device)
+        all_idx = torch.arange(self.centroids.shape[0], device=self.centroids.device)
         return self._rk4_ftle(all_idx, t0)

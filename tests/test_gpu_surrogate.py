@@ -231,7 +231,9 @@ def test_fused_inference_matches_layered_kernels(n):
         feat, tx, ty = mo.features(pts_np, net.freq_np, tangents=True)
         _, jx, jy = mo.jacobian(feat, tx, ty, Ws, bs)
         f_or = _ftle_from_tangents(jx, jy, net.out_scale, T)
-        assert _rel(f.cpu().numpy(), f_or) < 5e-3
+        # absolute: single-seed FTLEs can sit near 0, where a relative bound is
+        # meaningless; BF16 tangents move log(sigma) by ~1e-4 here, FTLE by ~1e-4/T
+        assert np.max(np.abs(f.cpu().numpy() - f_or)) < 1e-3
 
 
 def test_fused_inference_empty_and_errors():
@@ -296,3 +298,98 @@ def test_surrogate_judge_and_what_training_gains():
     loose = float(np.quantile(tr["rerr"], 0.5))
     assert np.mean(tr["rerr"] <= loose) >= 0.5
     assert np.mean(un["rerr"] <= loose) == 0.0
+
+
+# ---- 3D surrogate (input (x0, y0, z0, t0), hidden 384) ----------------------------------
+
+def _net3d(hidden=384, seed=21):
+    from pyftle_b200.surrogate import FlowMapMLP, fourier_frequencies
+    return FlowMapMLP(fourier_frequencies(32, dim=3, space_sigma=2.0, seed=seed),
+                      hidden=hidden, depth=4, out_scale=0.2, seed=seed)
+
+
+def test_3d_gradients_match_oracle():
+    net = _net3d()
+    rng = np.random.default_rng(22)
+    n = 512
+    pts = np.column_stack((rng.uniform(0, 2 * np.pi, (n, 3)), rng.uniform(0, 5, n)))
+    target = rng.normal(0, 1, (n, 3)).astype(np.float32)
+    loss = net.loss_and_grads(torch.from_numpy(pts).cuda(), torch.from_numpy(target).cuda())
+    torch.cuda.synchronize()
+    net.check_errors()
+    Ws = [net.weight(l, bf16=True).double().cpu().numpy()[:L.fan_out]
+          for l, L in enumerate(net.layers)]
+    bs = [net.bias(l).double().cpu().numpy()[:L.fan_out] for l, L in enumerate(net.layers)]
+    ref_loss, gW, gb, _ = mo.loss_and_grads(mo.features(pts, net.freq_np), Ws, bs,
+                                            target.astype(np.float64), 3)
+    assert float(loss.item()) == pytest.approx(ref_loss, rel=1e-3)
+    # the oracle rounds to BF16 at the GPU's points; FP32 (GPU) and FP64 (oracle) sums
+    # then land on different sides of a BF16 rounding boundary now and then (2^-8 each),
+    # and those flips compound back through four 384-wide layers: 5e-3 here
+    # (measured 2.3e-3 for the first layer) against 2e-3 for the 256-wide 2D network
+    for l, L in enumerate(net.layers):
+        assert _rel(net.grad_weight(l).double().cpu().numpy()[:L.fan_out], gW[l]) < 5e-3, l
+        assert _rel(net.grad_bias(l).double().cpu().numpy()[:L.fan_out], gb[l]) < 5e-3, l
+
+
+def test_3d_tangents_and_ftle_match_oracle():
+    net = _net3d(seed=23)
+    rng = np.random.default_rng(24)
+    n = 1000
+    pts = np.column_stack((rng.uniform(0, 2 * np.pi, (n, 3)), rng.uniform(0, 5, n)))
+    P = torch.from_numpy(pts).cuda()
+    y, jx, jy, jz = net.predict(P, jacobian=True)
+    Ws, bs = net.numpy_params()
+    Ws = [mo.bf16(w) for w in Ws]
+    feat, *tan = mo.features(pts, net.freq_np, tangents=True)
+    y_ref, J = mo.jacobian_n(feat, tan, Ws, bs)
+    assert _rel(y.double().cpu().numpy()[:, :3], y_ref) < 2e-3
+    for got, ref in zip((jx, jy, jz), J):
+        assert _rel(got.double().cpu().numpy()[:, :3], ref) < 5e-3
+    f = net.ftle(P, 2.0).cpu().numpy()
+    f_ref = mo.ftle_from_tangents(J, net.out_scale, 2.0)
+    assert _rel(f, f_ref) < 5e-3
+    end = net.end_positions(P).cpu().numpy()
+    np.testing.assert_allclose(end, pts[:, :3] + net.out_scale * y_ref, rtol=0, atol=2e-3)
+    torch.cuda.synchronize()
+    net.check_errors()
+
+
+def test_3d_surrogate_judge_and_what_training_gains():
+    from pyftle_b200 import SnapshotSeries, flows
+    from pyftle_b200.interpolate import GridSpec
+    from pyftle_b200.surrogate import FlowMapMLP, SurrogateFTLE, TrainConfig, fit_flow_map
+    n = 32
+    ax = flows.periodic_axis(n)
+    S = 16
+    dt = 2 * math.pi / S
+    snaps = flows.abc_snapshots(ax, ax, ax, np.arange(S) * dt)
+    grid = GridSpec.from_points(flows.grid_points_3d(ax, ax, ax), (n, n, n), periodic=True)
+    s64 = SnapshotSeries(grid, snaps, precision="fp64", periodic_time=True)
+    sfx = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+    h, T = 0.05, 1.0
+    starts = np.arange(4) * dt
+    from pyftle_b200.surrogate import fourier_frequencies
+    # the ABC field has only |k| = 1 modes: low spatial frequencies suit its flow map
+    freq = fourier_frequencies(32, dim=3, space_sigma=1.5, time_sigma=0.5, seed=2)
+    net, _ = fit_flow_map(s64, T=T, h=h, snapshot_dt=dt, t0_values=starts,
+                          num_samples=1 << 21, hidden=384, freq=freq,
+                          cfg=TrainConfig(steps=3000, batch=16384, lr=2e-3, warmup=50))
+    untrained = FlowMapMLP(net.freq_np, hidden=384, out_scale=net.out_scale, seed=9)
+    m = 16
+    sp = 2 * np.pi / m
+    errs = {}
+    for name, nn in (("trained", net), ("untrained", untrained)):
+        sur = SurrogateFTLE(nn, sfx, nx=m, ny=m, nz=m, origin=(0.5 * sp,) * 3,
+                            spacing=(sp,) * 3, T=T, h=h, snapshot_dt=dt, delta=1e-3, tile=8)
+        t0 = float(starts[1])
+        ref = sur.reference_field(t0)
+        fs, _, rerr = sur.evaluate(t0)
+        f, rep = sur.field(t0, tol=1e-3)
+        bad = torch.nonzero(torch.from_numpy(rep.region_errors).cuda() > 1e-3).squeeze(1)
+        rejected = torch.isin(sur.region_of, bad)
+        assert torch.equal(f[rejected], ref[rejected])
+        assert torch.equal(f[sur.sample_idx], ref[sur.sample_idx])
+        errs[name] = float(torch.linalg.vector_norm(fs - ref) / torch.linalg.vector_norm(ref))
+    print("3D raw FTLE error", errs)
+    assert errs["trained"] < 0.5 * errs["untrained"]

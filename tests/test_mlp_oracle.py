@@ -69,3 +69,37 @@ def test_tangents_match_finite_differences():
         yp = mo.forward(mo.features(pts + d, freq), Ws, bs, bf16_points=False)["Y"]
         ym = mo.forward(mo.features(pts - d, freq), Ws, bs, bf16_points=False)["Y"]
         np.testing.assert_allclose(j, (yp - ym) / (2 * eps), rtol=1e-5, atol=1e-8)
+
+
+def test_3d_tangents_and_ftle_match_finite_differences():
+    rng = np.random.default_rng(3)
+    F = 32
+    freq = np.zeros((F, 8), dtype=np.float32)
+    freq[:, :4] = rng.normal(0, 1.5, (F, 4))
+    dims = [2 * F, 48, 48, 3]
+    Ws = [rng.normal(0, 1.0 / np.sqrt(dims[i]), (dims[i + 1], dims[i])) for i in range(3)]
+    bs = [rng.normal(0, 0.1, dims[i + 1]) for i in range(3)]
+    pts = rng.uniform(0, 6.28, (6, 4))
+    feat, *tan = mo.features(pts, freq, tangents=True)
+    assert len(tan) == 3
+    _, J = mo.jacobian_n(feat, tan, Ws, bs, bf16_points=False)
+    eps = 1e-6
+    for a in range(3):
+        d = np.zeros(4)
+        d[a] = eps
+        yp = mo.forward(mo.features(pts + d, freq), Ws, bs, bf16_points=False)["Y"]
+        ym = mo.forward(mo.features(pts - d, freq), Ws, bs, bf16_points=False)["Y"]
+        np.testing.assert_allclose(J[a], (yp - ym) / (2 * eps), rtol=1e-5, atol=1e-8)
+    # FTLE of the map x + s*y(x) against finite differences of the map itself
+    s, T = 0.3, 2.0
+    f = mo.ftle_from_tangents(J, s, T)
+    h = 1e-6
+    Fd = np.zeros((6, 3, 3))
+    for a in range(3):
+        d = np.zeros(4)
+        d[a] = h
+        xp = pts[:, :3] + d[:3] + s * mo.forward(mo.features(pts + d, freq), Ws, bs, False)["Y"]
+        xm = pts[:, :3] - d[:3] + s * mo.forward(mo.features(pts - d, freq), Ws, bs, False)["Y"]
+        Fd[:, :, a] = (xp - xm) / (2 * h)
+    lam = np.linalg.eigvalsh(np.einsum("nra,nrb->nab", Fd, Fd))[:, -1]
+    np.testing.assert_allclose(f, np.log(np.sqrt(lam)) / T, rtol=1e-6)
