@@ -49,7 +49,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["abc", "batched", "gyre", "abc256", "surrogate"],
+    p.add_argument("--workload",
+                   choices=["abc", "batched", "gyre", "abc256", "surrogate", "surrogate3d"],
                    default="abc",
                    help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
                         "turbulence windows in one persistent launch")
@@ -857,6 +858,124 @@ def run_surrogate(args):
     return 0
 
 
+def run_surrogate3d(args):
+    """The 3D surrogate (input (x0, y0, z0, t0), 4 x 384 SiLU, BF16) on the ABC flow.
+
+    ABC on a periodic --grid^3 grid, 64 snapshots per period; windows of fixed
+    T = 2 (RK4 h = 0.02, 100 steps) starting at --sur-windows successive snapshot
+    times on a --sur-seeds^3 seed grid (delta 1e-3).  Training: --train-samples
+    FP64 RK4 trajectories, --train-steps Adam steps.  Each window: the surrogate form
+    (layered tcgen05 network + 3 Jacobian tangents, RK4 on 1% of every 16^3 region,
+    RK4 re-advection above --tol) against FX15 mixed RK4 (chunked, cell-sorted) on
+    every seed.
+    """
+    import torch
+
+    from pyftle_b200 import SnapshotSeries, flows
+    from pyftle_b200.interpolate import GridSpec
+    from pyftle_b200.surrogate import (SurrogateFTLE, TrainConfig, fit_flow_map,
+                                       fourier_frequencies)
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    L = 2 * math.pi
+    n, S = args.grid, 64
+    dt = L / S
+    h, T = 0.02, 2.0
+    ax = flows.periodic_axis(n)
+    snaps = flows.abc_snapshots_device(ax, ax, ax, np.arange(S) * dt)
+    grid = GridSpec.from_points(flows.grid_points_3d(ax, ax, ax), (n, n, n), periodic=True)
+    s64 = SnapshotSeries(grid, snaps, precision="fp64", periodic_time=True)
+    sfx = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+    del snaps
+    W = args.sur_windows
+    starts = np.arange(W) * dt
+    freq = fourier_frequencies(32, dim=3, space_sigma=1.5, time_sigma=0.5, seed=2)
+    net, fit = fit_flow_map(s64, T=T, h=h, snapshot_dt=dt, t0_values=starts,
+                            num_samples=args.train_samples, hidden=384, freq=freq,
+                            cfg=TrainConfig(steps=args.train_steps, batch=32768, lr=2e-3))
+    m = args.sur_seeds
+    sp = L / m
+    sur = SurrogateFTLE(net, sfx, nx=m, ny=m, nz=m, origin=(0.5 * sp,) * 3, spacing=(sp,) * 3,
+                        T=T, h=h, snapshot_dt=dt, delta=1e-3, tile=16, tol=args.tol,
+                        rk4_chunk_steps=50)
+    for t0 in starts[:min(args.warmup, W)]:
+        sur.field(float(t0))
+        sur.reference_field(float(t0))
+    torch.cuda.synchronize()
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    tols = sorted({args.tol, 3e-3, 1e-2, 3e-2, 1e-1})
+    t_sur = t_rk = t_eval = 0.0
+    raw_err, judged_err, acc = [], [], []
+    sweep = {t: {"accepted": [], "err_num": 0.0} for t in tols}
+    ref_norm2 = 0.0
+    readv_windows = 0
+    for t0 in starts:
+        t0 = float(t0)
+        e = [ev() for _ in range(4)]
+        e[0].record()
+        f, rep = sur.field(t0)
+        e[1].record()
+        ref = sur.reference_field(t0)
+        e[2].record()
+        fs, _, rerr = sur.evaluate(t0)
+        e[3].record()
+        torch.cuda.synchronize()
+        t_sur += e[0].elapsed_time(e[1])
+        t_rk += e[1].elapsed_time(e[2])
+        t_eval += e[2].elapsed_time(e[3])
+        rn = float(torch.linalg.vector_norm(ref))
+        ref_norm2 += rn * rn
+        judged_err.append(float(torch.linalg.vector_norm(f - ref)) / rn)
+        raw_err.append(float(torch.linalg.vector_norm(fs - ref)) / rn)
+        acc.append(rep.accepted_fraction)
+        readv_windows += int(rep.rejected > 0)
+        d = fs - ref
+        d[sur.sample_idx] = 0.0
+        for tl in tols:
+            ok = (rerr <= tl)[sur.region_of]
+            sweep[tl]["err_num"] += float(torch.sum((d * ok) ** 2))
+            sweep[tl]["accepted"].append(float((rerr <= tl).double().mean()))
+    eval_ms, rk_ms = t_eval / W, t_rk / W
+    sweep_out = []
+    for tl in tols:
+        a = float(np.mean(sweep[tl]["accepted"]))
+        est_ms = eval_ms + (1.0 - a) * rk_ms
+        sweep_out.append({"tol": tl, "accepted_regions": a,
+                          "ftle_rel_err_l2": math.sqrt(sweep[tl]["err_num"] / ref_norm2),
+                          "est_fields_per_s": 1e3 / est_ms,
+                          "est_speedup_vs_rk4": rk_ms / est_ms})
+    steps = int(round(T / h))
+    line = {
+        "metric": "FTLE fields/s, 3D surrogate form (1% RK4 judge, RK4 re-advection) vs RK4",
+        "value": W / (t_sur / 1e3), "unit": "fields/s", "n_gpus": 1, "steps": W,
+        "warmup": args.warmup, "ms_per_step": t_sur / W, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": f"ABC periodic {n}^3 grid, 64 snapshots/period; {W} windows "
+                               f"T=2 (RK4 h=0.02) on {m}^3 seeds x 6, delta 1e-3; judge tol "
+                               f"{args.tol:g} on 1% of each 16^3 region",
+                   "network": "64 Fourier features of (x0,y0,z0,t0) -> 4x384 SiLU -> 3, BF16",
+                   "training": fit},
+        "rk4_fields_per_s": W / (t_rk / 1e3),
+        "rk4_particle_steps_per_s": 6 * m ** 3 * steps * W / (t_rk / 1e3),
+        "speedup_vs_rk4": t_rk / t_sur,
+        "accepted_regions_mean": float(np.mean(acc)),
+        "ftle_rel_err_l2_raw_surrogate_vs_rk4": {"max": max(raw_err), "mean": float(np.mean(raw_err))},
+        "ftle_rel_err_l2_judged_vs_rk4": {"max": max(judged_err), "mean": float(np.mean(judged_err))},
+        "surrogate_and_judge_ms_per_field": eval_ms, "rk4_ms_per_field": rk_ms,
+        "tolerance_sweep": sweep_out,
+        # per window: per 2^20-seed chunk the feature kernel, 4 primal + 1 output GEMM,
+        # 3 tangent passes of 5 GEMMs and the FTLE kernel (22); the judge's RK4 window
+        # (2 chunk launches + one 3-kernel cell sort); the same again when any region
+        # is re-advected
+        "gpu_launches": W * (22 * (-(-m ** 3 // (1 << 20))) + 5) + 5 * readv_windows,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.workload == "abc256" and args.impl != "reference":
@@ -869,6 +988,8 @@ def main():
         return run_gyre(args)
     if args.workload == "surrogate":
         return run_surrogate(args)
+    if args.workload == "surrogate3d":
+        return run_surrogate3d(args)
     return run_ours(args)
 
 
