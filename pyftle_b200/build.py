@@ -2,8 +2,9 @@
 
 Each CUDA source is compiled on its own so it can carry its own FP flags:
 ``plain_f64.cu`` is built with ``-fmad=false`` (no FMA contraction: the FP64
-path reproduces pyFTLE's rounding step by step); the mixed-precision and
-plumbing sources keep FMA contraction on.  The CUDA runtime is linked
+path reproduces pyFTLE's rounding step by step), and so is ``mixed.cu``: every
+FMA it intends is written as ``fmaf``/``fma``, so its results do not depend on
+where the compiler would otherwise fuse a product into a sum.  The CUDA runtime is linked
 statically so the library has no dependency beyond the driver.
 
 Usage: ``python -m pyftle_b200.build [--force] [--verbose]``.
@@ -29,7 +30,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relax
 SOURCES = {
     "api.cu": [],
     "plain_f64.cu": ["-fmad=false"],
-    "mixed.cu": [],
+    "mixed.cu": ["-fmad=false"],
     "no_alloc.cu": [],
     "mlp.cu": [],
     "mlp_fused.cu": [],

@@ -471,7 +471,7 @@ struct WarpQueue {
 template <int DIM, int STORAGE, bool BLEND>
 __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
                                            const unsigned char *__restrict__ recs, float alpha,
-                                           const double *cs, const float (*d)[DIM],
+                                           const double *cs, const float *d,
                                            float (*kd)[DIM], float as, float *uc,
                                            float *slots_base, WarpQueue<DIM> &wq, int lane) {
   constexpr int K = 2 * DIM;
@@ -510,8 +510,10 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
     bool same = true;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
-      dl[a] = fmaf(as, kd[k][a], d[k][a]) * m.inv_spf[a];
-      F[a] = fc[a] + dl[a];
+      // explicit roundings: the cell test and the polynomial use the same F and dl
+      // whatever the compiler schedules (no contraction into one FMA)
+      dl[a] = __fmul_rn(fmaf(as, kd[k][a], d[(k * DIM + a) * kBlock]), m.inv_spf[a]);
+      F[a] = __fadd_rn(fc[a], dl[a]);
       same = same && F[a] >= 0.0f && F[a] < 1.0f;
     }
 #pragma unroll
@@ -591,8 +593,7 @@ template <int DIM>
 struct GroupState {
   double c[DIM];            // centroid (periodic grids: inside the primary period)
   int wraps[DIM];           // periods removed from the centroid
-  float d[2 * DIM][DIM];    // neighbour offsets
-  double id[DIM];           // initial diagonal separations (Jacobian denominators)
+  float d[2 * DIM][DIM];    // neighbour offsets (in shared memory during the step loop)
   float kcp[DIM];           // AB2: previous centroid velocity
   float kdp[2 * DIM][DIM];  // AB2: previous velocity differences
 };
@@ -623,8 +624,6 @@ __device__ __forceinline__ void group_from_positions(const MixK &m, const WinVar
       st.kdp[k][a] = 0.0f;
     }
 #pragma unroll
-  for (int j = 0; j < DIM; ++j) st.id[j] = X[plus_r(j)][j] - X[minus_r(j)][j];
-#pragma unroll
   for (int a = 0; a < DIM; ++a) {
     st.kcp[a] = 0.0f;
     st.wraps[a] = 0;
@@ -642,8 +641,8 @@ __device__ __forceinline__ void group_from_positions(const MixK &m, const WinVar
 template <int DIM, int MODE, int INTEG, int STORAGE>
 __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, const Header16 &hd,
                                              GroupState<DIM> &st, int i0, int i1,
-                                             float *smem_slots, float *acc, WarpQueue<DIM> &wq,
-                                             int lane) {
+                                             float *smem_slots, float *acc, float *dsm,
+                                             WarpQueue<DIM> &wq, int lane) {
   constexpr int K = 2 * DIM;
   constexpr bool BLEND = MODE == FTLE_BLEND;
   const bool periodic = m.w.g.periodic != 0;
@@ -656,6 +655,12 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
   for (int k = 0; k < K; ++k)
 #pragma unroll
     for (int a = 0; a < DIM; ++a) kd[k][a] = 0.0f;
+  // the offsets live in this thread's shared-memory column during the step loop,
+  // which frees 3*K registers (the kernel then fits 4 blocks per SM)
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) dsm[(k * DIM + a) * kBlock] = st.d[k][a];
 
   constexpr int NST = INTEG == FTLE_RK4 ? 4 : 1;
   for (int i = i0; i < i1; ++i) {
@@ -673,7 +678,7 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
 #pragma unroll
       for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], st.c[a]);
       float uc[DIM];
-      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, st.d, kd, as, uc, smem_slots, wq,
+      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, dsm, kd, as, uc, smem_slots, wq,
                                       lane);
 #pragma unroll
       for (int a = 0; a < DIM; ++a) {
@@ -699,14 +704,16 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
       for (int k = 0; k < K; ++k)
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
-          st.d[k][a] = fmaf(h6f, acc[(k * DIM + a) * kBlock], st.d[k][a]);
+          dsm[(k * DIM + a) * kBlock] =
+              fmaf(h6f, acc[(k * DIM + a) * kBlock], dsm[(k * DIM + a) * kBlock]);
     } else if constexpr (INTEG == FTLE_EULER) {
 #pragma unroll
       for (int a = 0; a < DIM; ++a) st.c[a] = fma(h, (double)kc[a], st.c[a]);
 #pragma unroll
       for (int k = 0; k < K; ++k)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) st.d[k][a] = fmaf(hf, kd[k][a], st.d[k][a]);
+        for (int a = 0; a < DIM; ++a)
+          dsm[(k * DIM + a) * kBlock] = fmaf(hf, kd[k][a], dsm[(k * DIM + a) * kBlock]);
     } else {  // AB2, Euler on the first step (integrate.py:240-246)
       if (i == 0) {
 #pragma unroll
@@ -714,7 +721,8 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
 #pragma unroll
         for (int k = 0; k < K; ++k)
 #pragma unroll
-          for (int a = 0; a < DIM; ++a) st.d[k][a] = fmaf(hf, kd[k][a], st.d[k][a]);
+          for (int a = 0; a < DIM; ++a)
+            dsm[(k * DIM + a) * kBlock] = fmaf(hf, kd[k][a], dsm[(k * DIM + a) * kBlock]);
       } else {
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
@@ -723,7 +731,8 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
         for (int k = 0; k < K; ++k)
 #pragma unroll
           for (int a = 0; a < DIM; ++a)
-            st.d[k][a] = fmaf(hf, fmaf(1.5f, kd[k][a], -0.5f * st.kdp[k][a]), st.d[k][a]);
+            dsm[(k * DIM + a) * kBlock] =
+                fmaf(hf, fmaf(1.5f, kd[k][a], -0.5f * st.kdp[k][a]), dsm[(k * DIM + a) * kBlock]);
       }
 #pragma unroll
       for (int a = 0; a < DIM; ++a) st.kcp[a] = kc[a];
@@ -747,6 +756,10 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
       }
     }
   }
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) st.d[k][a] = dsm[(k * DIM + a) * kBlock];
 }
 
 // Final positions x_k = c + wraps*period + d_k and the FP64 FTLE epilogue.
@@ -759,6 +772,13 @@ __device__ __forceinline__ void group_finish(const MixK &m, const WinVar &v, lon
 #pragma unroll
   for (int a = 0; a < DIM; ++a)
     c[a] = m.w.g.periodic ? st.c[a] + (double)st.wraps[a] * m.period[a] : st.c[a];
+  // initial diagonal separations (Jacobian denominators), read from the seeds before
+  // this group's final positions overwrite them
+  double id[DIM];
+#pragma unroll
+  for (int j = 0; j < DIM; ++j)
+    id[j] = v.positions[((long long)plus_r(j) * N + g) * DIM + j] -
+            v.positions[((long long)minus_r(j) * N + g) * DIM + j];
   if (!v.keep_positions) {
 #pragma unroll
     for (int k = 0; k < K; ++k)
@@ -772,7 +792,7 @@ __device__ __forceinline__ void group_finish(const MixK &m, const WinVar &v, lon
     for (int i = 0; i < DIM; ++i)
 #pragma unroll
       for (int j = 0; j < DIM; ++j)
-        J[i][j] = ((double)st.d[plus_r(j)][i] - (double)st.d[minus_r(j)][i]) / st.id[j];
+        J[i][j] = ((double)st.d[plus_r(j)][i] - (double)st.d[minus_r(j)][i]) / id[j];
     double lam;
     if constexpr (DIM == 2) {
       lam = lmax2(J[0][0], J[0][1], J[1][0], J[1][1]);
@@ -797,7 +817,6 @@ struct ChunkBuf {
   double *c;      // DIM x N
   int *wraps;     // DIM x N
   float *d;       // K*DIM x N
-  double *id;     // DIM x N
   float *hist;    // (DIM + K*DIM) x N, AB2 only
   long long *idx; // N: original group index
 };
@@ -810,7 +829,6 @@ __device__ __forceinline__ void state_load(const ChunkBuf &b, long long N, long 
   for (int a = 0; a < DIM; ++a) {
     st.c[a] = b.c[a * N + j];
     st.wraps[a] = b.wraps[a * N + j];
-    st.id[a] = b.id[a * N + j];
     st.kcp[a] = ab2 ? b.hist[a * N + j] : 0.0f;
   }
 #pragma unroll
@@ -830,7 +848,6 @@ __device__ __forceinline__ void state_store(const ChunkBuf &b, long long N, long
   for (int a = 0; a < DIM; ++a) {
     b.c[a * N + j] = st.c[a];
     b.wraps[a * N + j] = st.wraps[a];
-    b.id[a * N + j] = st.id[a];
     if (ab2) b.hist[a * N + j] = st.kcp[a];
   }
 #pragma unroll
@@ -908,7 +925,6 @@ __global__ void sort_scatter_kernel(const int *__restrict__ keys, long long N, i
     for (int a = 0; a < DIM; ++a) {
       out.c[a * N + p] = in.c[a * N + j];
       out.wraps[a * N + p] = in.wraps[a * N + j];
-      out.id[a * N + p] = in.id[a * N + j];
     }
 #pragma unroll
     for (int q = 0; q < K * DIM; ++q) out.d[q * N + p] = in.d[q * N + j];
@@ -926,17 +942,35 @@ __global__ void sort_scatter_kernel(const int *__restrict__ keys, long long N, i
 // comes from the role-blocked positions (slot = group index); last: final
 // positions and FTLE are written at the group's original index; otherwise
 // the state goes back to `buf` (and its cell key to `keys` when given).
+// Shared memory of a block (dynamic): per-thread columns of the off-cell slots, the
+// RK4 accumulators and the offsets (K*DIM floats each, stride kBlock), then one
+// gather queue per warp.
+template <int DIM>
+struct BlockSmem {
+  static constexpr int kCol = 2 * DIM * DIM * kBlock;
+  static constexpr size_t kBytes = 3 * kCol * sizeof(float) + (kBlock / 32) * sizeof(WarpQueue<DIM>);
+  float *slots, *acc, *d;
+  WarpQueue<DIM> *queue;
+  __device__ explicit BlockSmem(unsigned char *base) {
+    float *f = reinterpret_cast<float *>(base);
+    slots = f;
+    acc = f + kCol;
+    d = f + 2 * kCol;
+    queue = reinterpret_cast<WarpQueue<DIM> *>(f + 3 * kCol);
+  }
+};
+
 template <int DIM, int MODE, int INTEG, int STORAGE>
-__global__ void __launch_bounds__(kBlock, 3)
+__global__ void __launch_bounds__(kBlock, 4)
     window_mixed_kernel(const MixK m, const ChunkBuf buf, int i0, int i1, int first, int last,
                         int *keys, int key_bits) {
-  constexpr int K = 2 * DIM;
-  __shared__ float smem_slots[K * DIM * kBlock];
-  __shared__ float smem_acc[K * DIM * kBlock];  // RK4 accumulators of the offsets
-  __shared__ WarpQueue<DIM> smem_queue[kBlock / 32];
-  float *acc = smem_acc + threadIdx.x;
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  const BlockSmem<DIM> sm(dyn_smem);
+  float *smem_slots = sm.slots;
+  float *acc = sm.acc + threadIdx.x;
+  float *dsm = sm.d + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  WarpQueue<DIM> &wq = smem_queue[threadIdx.x >> 5];
+  WarpQueue<DIM> &wq = sm.queue[threadIdx.x >> 5];
   const long long N = m.w.N;
   const long long j_raw = (long long)blockIdx.x * kBlock + threadIdx.x;
   // lanes past the end mirror the last slot (warp-wide shuffles need every lane) but write nothing
@@ -955,7 +989,7 @@ __global__ void __launch_bounds__(kBlock, 3)
     g = buf.idx[j];
     state_load<DIM>(buf, N, j, st, AB2);
   }
-  group_advect<DIM, MODE, INTEG, STORAGE>(m, v, hd, st, i0, i1, smem_slots, acc, wq, lane);
+  group_advect<DIM, MODE, INTEG, STORAGE>(m, v, hd, st, i0, i1, smem_slots, acc, dsm, wq, lane);
   if (!active) return;
   if (last) {
     group_finish<DIM>(m, v, g, st);
@@ -994,17 +1028,17 @@ static int64_t plan_total(int nw, int64_t ni) { return plan_offset_counter(nw, n
 // Persistent CTAs take work items from a global counter until the list is empty;
 // every thread of an item advects one group of that item's window.
 template <int DIM, int MODE, int INTEG, int STORAGE>
-__global__ void __launch_bounds__(kBlock, 3)
+__global__ void __launch_bounds__(kBlock, 4)
     windows_persistent_kernel(const MixK m, const WinVar *__restrict__ wins,
                               const BatchItem *__restrict__ items, int num_items, int *counter) {
-  constexpr int K = 2 * DIM;
-  __shared__ float smem_slots[K * DIM * kBlock];
-  __shared__ float smem_acc[K * DIM * kBlock];
-  __shared__ WarpQueue<DIM> smem_queue[kBlock / 32];
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  const BlockSmem<DIM> sm(dyn_smem);
   __shared__ int s_item;
-  float *acc = smem_acc + threadIdx.x;
+  float *smem_slots = sm.slots;
+  float *acc = sm.acc + threadIdx.x;
+  float *dsm = sm.d + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  WarpQueue<DIM> &wq = smem_queue[threadIdx.x >> 5];
+  WarpQueue<DIM> &wq = sm.queue[threadIdx.x >> 5];
   const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -1019,19 +1053,32 @@ __global__ void __launch_bounds__(kBlock, 3)
     const long long j = active ? j_raw : v.N - 1;
     GroupState<DIM> st;
     group_from_positions<DIM>(m, v, j, st);
-    group_advect<DIM, MODE, INTEG, STORAGE>(m, v, hd, st, 0, v.num_steps, smem_slots, acc, wq,
-                                            lane);
+    group_advect<DIM, MODE, INTEG, STORAGE>(m, v, hd, st, 0, v.num_steps, smem_slots, acc, dsm,
+                                            wq, lane);
     if (active) group_finish<DIM>(m, v, j, st);
   }
+}
+
+// Allow the kernel's dynamic shared memory (the 3D block needs the full 48 KB plus the
+// persistent kernel's work-item word); called once per kernel instance.
+template <typename Kernel>
+static bool set_smem_attr(Kernel kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  return true;
 }
 
 template <int DIM, int MODE, int STORAGE>
 static void launch_persistent(const MixK &m, int integ, const WinVar *wins,
                               const BatchItem *items, int num_items, int *counter, int ctas,
                               cudaStream_t st) {
-#define LP(I)                                                                        \
-  windows_persistent_kernel<DIM, MODE, I, STORAGE><<<ctas, kBlock, 0, st>>>(m, wins, items, \
-                                                                          num_items, counter)
+#define LP(I)                                                                              \
+  do {                                                                                     \
+    static const bool attr_set = set_smem_attr(windows_persistent_kernel<DIM, MODE, I, STORAGE>, \
+                                               BlockSmem<DIM>::kBytes);                    \
+    (void)attr_set;                                                                        \
+    windows_persistent_kernel<DIM, MODE, I, STORAGE>                                       \
+        <<<ctas, kBlock, BlockSmem<DIM>::kBytes, st>>>(m, wins, items, num_items, counter); \
+  } while (0)
   if (integ == FTLE_EULER)
     LP(FTLE_EULER);
   else if (integ == FTLE_AB2)
@@ -1071,9 +1118,14 @@ template <int DIM, int MODE, int STORAGE>
 static void launch_mixed(const MixK &m, int integ, const ChunkBuf &buf, int i0, int i1,
                          int first, int last, int *keys, int key_bits, cudaStream_t st) {
   const unsigned blocks = (unsigned)((m.w.N + kBlock - 1) / kBlock);
-#define LM(I)                                                                             \
-  window_mixed_kernel<DIM, MODE, I, STORAGE><<<blocks, kBlock, 0, st>>>(m, buf, i0, i1, first, \
-                                                                         last, keys, key_bits)
+#define LM(I)                                                                            \
+  do {                                                                                   \
+    static const bool attr_set =                                                         \
+        set_smem_attr(window_mixed_kernel<DIM, MODE, I, STORAGE>, BlockSmem<DIM>::kBytes); \
+    (void)attr_set;                                                                      \
+    window_mixed_kernel<DIM, MODE, I, STORAGE><<<blocks, kBlock, BlockSmem<DIM>::kBytes, st>>>( \
+        m, buf, i0, i1, first, last, keys, key_bits);                                    \
+  } while (0)
   if (integ == FTLE_EULER)
     LM(FTLE_EULER);
   else if (integ == FTLE_AB2)
@@ -1151,7 +1203,6 @@ static WsLayout ws_layout(int dim, int integ, int64_t N) {
   per += align256(8 * dim * N);                 // c
   per += align256(4 * dim * N);                 // wraps
   per += align256(4 * K * dim * N);             // d
-  per += align256(8 * dim * N);                 // id
   per += integ == FTLE_AB2 ? align256(4 * (dim + K * dim) * N) : 0;  // AB2 history
   per += align256(8 * N);                       // idx
   L.state_bytes = per;
@@ -1173,8 +1224,6 @@ static ChunkBuf carve(unsigned char *base, int dim, int integ, int64_t N) {
   p += align256(4 * dim * N);
   b.d = reinterpret_cast<float *>(p);
   p += align256(4 * K * dim * N);
-  b.id = reinterpret_cast<double *>(p);
-  p += align256(8 * dim * N);
   if (integ == FTLE_AB2) {
     b.hist = reinterpret_cast<float *>(p);
     p += align256(4 * (dim + K * dim) * N);
