@@ -211,7 +211,8 @@ int ftle_analytic_window_run(const ftle_flow *flow, int32_t integrator, double t
  * work list; order 1 = longest windows first, 0 = as given), copy it to a
  * 256-byte aligned device buffer, then run it any number of times; the plan
  * holds the windows' device pointers.  The run only issues a memset of the
- * plan's counter and one kernel on `stream`. */
+ * plan's counter and one kernel on `stream` (ctas_per_sm x 148 persistent CTAs,
+ * ctas_per_sm in 1..8; 4 blocks per SM are resident in 3D, 8 in 2D). */
 int64_t ftle_windows_plan_bytes(const ftle_window *windows, int32_t count);
 int ftle_windows_plan(const ftle_window *windows, int32_t count, int32_t order,
                       void *host_plan, int64_t plan_bytes);

@@ -48,7 +48,7 @@ class WindowSpecRun:
 
 @dataclass(frozen=True)
 class Schedule:
-    ctas_per_sm: int = 3
+    ctas_per_sm: int = 4  # the kernel fits 4 blocks of 128 threads per SM
     order: int = 1  # 1: longest windows first, 0: as given
 
 
@@ -147,7 +147,9 @@ class WindowBatch:
         if use_cache and self.shape_key in cache:
             self.schedule = Schedule(**cache[self.shape_key]["schedule"])
             return self.schedule
-        cands = list(candidates) if candidates else [Schedule(c, o) for c in (1, 2, 3)
+        # blocks per SM the kernel can keep resident: 4 in 3D, up to 8 in 2D
+        ctas = (1, 2, 3, 4) if self.series.grid.dim == 3 else (2, 4, 6, 8)
+        cands = list(candidates) if candidates else [Schedule(c, o) for c in ctas
                                                      for o in (1, 0)]
         timings = []
         for sch in cands:

@@ -85,14 +85,18 @@ struct Dec<FTLE_FX15> {
 // packing (S, dim, nodes) float64 -> header + pair records
 // ---------------------------------------------------------------------------
 
+// Float min/max through integer atomics: a float with the sign bit clear orders like
+// its bits as a signed int, one with the sign bit set orders reversed as unsigned.
+// The branch tests the sign BIT, so -0.0 takes the negative path (as a signed int its
+// bits are INT_MIN and would replace any true negative minimum).
 __device__ __forceinline__ void atomic_min_f(float *a, float v) {
-  if (v >= 0.0f)
+  if (__float_as_int(v) >= 0)
     atomicMin(reinterpret_cast<int *>(a), __float_as_int(v));
   else
     atomicMax(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
 }
 __device__ __forceinline__ void atomic_max_f(float *a, float v) {
-  if (v >= 0.0f)
+  if (__float_as_int(v) >= 0)
     atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
   else
     atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
@@ -945,6 +949,16 @@ __global__ void sort_scatter_kernel(const int *__restrict__ keys, long long N, i
 // Shared memory of a block (dynamic): per-thread columns of the off-cell slots, the
 // RK4 accumulators and the offsets (K*DIM floats each, stride kBlock), then one
 // gather queue per warp.
+// Blocks of kBlock threads resident per SM that the register budget is sized for
+// (measured on B200): 4 in 3D; in 2D the persistent batched kernel runs 8 (the
+// turbulence windows keep most neighbours in their cell and gain from latency
+// hiding), the single-window kernel 4 (long, strongly stretching windows gather
+// per neighbour and need the L1 that a larger shared-memory carve-out takes).
+template <int DIM>
+constexpr int kMinBlocks = 4;
+template <int DIM>
+constexpr int kMinBlocksPersistent = DIM == 2 ? 8 : 4;
+
 template <int DIM>
 struct BlockSmem {
   static constexpr int kCol = 2 * DIM * DIM * kBlock;
@@ -961,7 +975,7 @@ struct BlockSmem {
 };
 
 template <int DIM, int MODE, int INTEG, int STORAGE>
-__global__ void __launch_bounds__(kBlock, 4)
+__global__ void __launch_bounds__(kBlock, kMinBlocks<DIM>)
     window_mixed_kernel(const MixK m, const ChunkBuf buf, int i0, int i1, int first, int last,
                         int *keys, int key_bits) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -1028,7 +1042,7 @@ static int64_t plan_total(int nw, int64_t ni) { return plan_offset_counter(nw, n
 // Persistent CTAs take work items from a global counter until the list is empty;
 // every thread of an item advects one group of that item's window.
 template <int DIM, int MODE, int INTEG, int STORAGE>
-__global__ void __launch_bounds__(kBlock, 4)
+__global__ void __launch_bounds__(kBlock, kMinBlocksPersistent<DIM>)
     windows_persistent_kernel(const MixK m, const WinVar *__restrict__ wins,
                               const BatchItem *__restrict__ items, int num_items, int *counter) {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
@@ -1411,7 +1425,7 @@ int ftle_windows_run_mixed(const ftle_window *windows, int32_t count, void *devi
     return fail_invalid("plan buffer too small: need %lld bytes", (long long)plan_total(count, ni));
   if (reinterpret_cast<uintptr_t>(device_plan) % 256 != 0)
     return fail_invalid("plan must be 256-byte aligned");
-  if (ctas_per_sm < 1 || ctas_per_sm > 3) return fail_invalid("ctas_per_sm must be 1, 2 or 3");
+  if (ctas_per_sm < 1 || ctas_per_sm > 8) return fail_invalid("ctas_per_sm must be 1 to 8");
   if (ni == 0) return FTLE_OK;
   MixK m;
   mixed_setup(&windows[0], m);

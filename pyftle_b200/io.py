@@ -148,6 +148,9 @@ def load_snapshots(files: Sequence[str], dim: int, nodes: int, workers: int = 8,
     device = device or torch.device("cuda", torch.cuda.current_device())
     out = torch.empty((len(files), dim, nodes), dtype=torch.float64, device=device)
     copy_stream = torch.cuda.Stream(device=device)
+    # `out` comes from the current stream's pool: work still queued there may own
+    # its memory until it finishes, so the copies wait for that work first
+    copy_stream.wait_stream(torch.cuda.current_stream(device))
     staging: List[torch.Tensor] = []
 
     def read(path):

@@ -422,3 +422,25 @@ def test_keep_positions_leaves_seeds_and_same_ftle(precision):
     f2 = run_window(series, p2, keep_positions=True, **kw)
     np.testing.assert_array_equal(host(p2), pos)
     np.testing.assert_array_equal(host(f2), host(f1))
+
+
+def test_fx15_range_is_exact_and_repeatable_with_negative_zeros():
+    """The FX15 value range (per-component min / max over the series) must not depend
+    on the order of the device's atomic updates; exact -0.0 values (a velocity field
+    vanishing on a boundary) once let a min of -0.0 override a negative minimum."""
+    rng = np.random.default_rng(3)
+    nx, ny, S = 250, 200, 6
+    snaps = rng.uniform(-1.0, 1.0, (S, 2, nx * ny))
+    snaps[:, :, ::7] = -0.0
+    grid = GridSpec(shape=(nx, ny), origin=(0.0, 0.0), spacing=(1.0, 1.0))
+    headers = []
+    for _ in range(5):
+        series = SnapshotSeries(grid, snaps, precision="fx15")
+        headers.append(np.frombuffer(series.packed[:64].cpu().numpy().tobytes(), np.float32))
+    for h in headers[1:]:
+        np.testing.assert_array_equal(h, headers[0])
+    vmin, vmax = headers[0][8:10], headers[0][12:14]
+    for c in range(2):
+        lo, hi = snaps[:, c].min(), snaps[:, c].max()
+        assert vmin[c] <= lo and np.nextafter(vmin[c], np.float32(np.inf)) > lo
+        assert vmax[c] >= hi and np.nextafter(vmax[c], np.float32(-np.inf)) < hi
