@@ -63,6 +63,10 @@ def parse_args():
     p.add_argument("--windows", type=int, default=32, help="abc256: number of windows")
     p.add_argument("--urms", type=float, default=0.02,
                    help="batched workload: rms speed of the turbulence field")
+    p.add_argument("--batch-snapshots", type=int, default=400,
+                   help="batched workload: snapshots in the series (a smaller case for profiling)")
+    p.add_argument("--batch-max-length", type=float, default=20.0,
+                   help="batched workload: window lengths are uniform in [max/10, max]")
     p.add_argument("--chunk-steps", type=int, default=50,
                    help="mixed path: steps per launch between cell sorts (0: one launch)")
     p.add_argument("--sort-every", type=int, default=1)
@@ -470,6 +474,7 @@ def run_batched(args):
     1024^2 periodic grid over [0, 2pi)^2, 400 FX15 snapshots at dt = 0.05; window i:
     seed grid nx x nx/2 with nx log-uniform in [64, 1024], length U[2, 20], start
     uniform in [0, 20 - length], RK4 h = 0.025, 4 neighbours at delta = 5e-4.
+    ``--batch-snapshots`` / ``--batch-max-length`` shrink it for profiling.
     """
     import torch
 
@@ -479,7 +484,7 @@ def run_batched(args):
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     rng = np.random.default_rng(2026)
-    n, S, dt, h = 1024, 400, 0.05, 0.025
+    n, S, dt, h = 1024, args.batch_snapshots, 0.05, 0.025
     L = 2 * math.pi
     turb = flows.FourierTurbulence2D(seed=7, num_modes=256, kmin=4, kmax=128, urms=args.urms)
     t_gen = time.time()
@@ -494,7 +499,7 @@ def run_batched(args):
     for i in range(64):
         nx = int(round(math.exp(rng.uniform(math.log(64), math.log(1024)))))
         ny = max(1, nx // 2)
-        length = rng.uniform(2.0, 20.0)
+        length = rng.uniform(0.1 * args.batch_max_length, args.batch_max_length)
         steps = int(round(length / h))
         t0 = rng.uniform(0.0, (S - 1) * dt - steps * h)
         cx = (np.arange(nx) + 0.5) * (L / nx)
@@ -548,9 +553,10 @@ def run_batched(args):
         "metric": METRIC + " (batched windows)", "value": value, "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "64 uneven 2D turbulence windows, 1024^2 periodic grid, 400 "
-                               "snapshots, seed grids 64x32..1024x512, lengths U[2,20], RK4 "
-                               "h=0.025, one persistent CUDA-graph launch",
+        "config": {"workload": f"64 uneven 2D turbulence windows, 1024^2 periodic grid, {S} "
+                               f"snapshots, seed grids 64x32..1024x512, lengths "
+                               f"U[{0.1 * args.batch_max_length:g},{args.batch_max_length:g}], "
+                               f"RK4 h=0.025, one persistent CUDA-graph launch",
                    "precision": series.precision, "windows": 64, "urms": args.urms,
                    "particles": sum(w.positions.shape[0] for w in wins),
                    "particle_steps": ps, "schedule": {"ctas_per_sm": best.ctas_per_sm,

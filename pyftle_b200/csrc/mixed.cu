@@ -459,13 +459,14 @@ __device__ __forceinline__ double lmax2(double F00, double F01, double F10, doub
 }
 
 
-// Off-cell neighbour work items of one warp (structure of arrays, per warp).
+// Off-cell neighbour work items of one warp.  An item is the slot index of the
+// owning thread's neighbour (its in-cell coordinates F relative to the owner's
+// centroid cell wait in that slot); the owners' centroid cells sit beside it.
 template <int DIM>
 struct WarpQueue {
   static constexpr int kCap = 32 * 2 * DIM;
-  int cell[DIM][kCap];
-  float q[DIM][kCap];
-  int dst[kCap];  // slot index of the owning thread's neighbour
+  int dst[kCap];
+  int ci[DIM][32];  // centroid cell of each lane's group
 };
 
 // Per stage: centroid velocity uc and, in place of the previous stage's kd[k], the
@@ -525,11 +526,20 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
       const float dp = poly_diff<DIM>(A[c], fc, dl, F);
       kd[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
     }
-    if (!same) {
+    // 2D stores every neighbour's F without a branch (most warps have an off-cell
+    // neighbour in most stages); 3D stores only the off-cell ones (measured faster)
+    if constexpr (DIM == 2) {
+      off |= (!same && ok) ? 1u << k : 0u;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
+    } else if (!same && ok) {
       off |= 1u << k;
 #pragma unroll
       for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
     }
+  }
+  if constexpr (DIM == 2) {
+    if (!__any_sync(0xffffffffu, off != 0u)) return;
   }
   // pass 2: queue the off-cell neighbours of the whole warp
   const int cnt = __popc(off);
@@ -544,34 +554,30 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
   __syncwarp();  // every lane has read its slots of the previous stage
   int pos = incl - cnt;
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    if (off & (1u << k)) {
+  for (int a = 0; a < DIM; ++a) wq.ci[a][lane] = ci[a];
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) {
-        const float F = slots[(k * DIM + a) * kBlock];
-        const float fo = floorf(F);
-        wq.cell[a][pos] = ci[a] + (int)fo;
-        wq.q[a][pos] = F - fo;
-      }
-      wq.dst[pos] = k * DIM * kBlock + (int)threadIdx.x;
-      ++pos;
-    }
+  for (int k = 0; k < K; ++k) {
+    if (off & (1u << k)) wq.dst[pos++] = k * DIM * kBlock + (int)threadIdx.x;
   }
   __syncwarp();
-  // pass 3: 32 queued gathers at a time
+  // pass 3: 32 queued gathers at a time (a group whose centroid is not finite queues
+  // nothing, so every item belongs to a valid group)
   for (int b = 0; b < total; b += 32) {
     const int it = b + lane;
     if (it < total) {
+      const int dst = wq.dst[it];
+      const int owner = dst & 31;  // the owner's lane (blocks are whole warps)
       int cell[DIM];
       float q[DIM];
 #pragma unroll
       for (int a = 0; a < DIM; ++a) {
-        cell[a] = wq.cell[a][it];
-        q[a] = wq.q[a][it];
+        const float F = slots_base[dst + a * kBlock];
+        const float fo = floorf(F);
+        cell[a] = wq.ci[a][owner] + (int)fo;
+        q[a] = F - fo;
       }
       float v[DIM][NC];
-      const bool kin = ok && cell_values<DIM, STORAGE, BLEND>(m, recs, alpha, cell, v);
-      const int dst = wq.dst[it];
+      const bool kin = cell_values<DIM, STORAGE, BLEND>(m, recs, alpha, cell, v);
 #pragma unroll
       for (int c = 0; c < DIM; ++c) {
         const float p = interp_lerp<DIM>(v[c], q);
@@ -582,7 +588,13 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
   __syncwarp();
 #pragma unroll
   for (int k = 0; k < K; ++k) {
-    if (off & (1u << k)) {
+    if constexpr (DIM == 2) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        const float sv = slots[(k * DIM + c) * kBlock] - uc[c];
+        kd[k][c] = (off & (1u << k)) ? sv : kd[k][c];
+      }
+    } else if (off & (1u << k)) {
 #pragma unroll
       for (int c = 0; c < DIM; ++c) kd[k][c] = slots[(k * DIM + c) * kBlock] - uc[c];
     }
