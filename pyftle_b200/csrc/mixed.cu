@@ -1085,8 +1085,9 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPersistent<DIM>)
   }
 }
 
-// Allow the kernel's dynamic shared memory (the 3D block needs the full 48 KB plus the
-// persistent kernel's work-item word); called once per kernel instance.
+// Allow the kernel's dynamic shared memory (31.5 KB for a 3D block, 15 KB in 2D, under
+// the 48 KB default today; set anyway so a larger layout needs no other change);
+// called once per kernel instance.
 template <typename Kernel>
 static bool set_smem_attr(Kernel kernel, size_t bytes) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

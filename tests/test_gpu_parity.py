@@ -424,6 +424,41 @@ def test_keep_positions_leaves_seeds_and_same_ftle(precision):
     np.testing.assert_array_equal(host(f2), host(f1))
 
 
+@pytest.mark.parametrize("chunk", [None, 10])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_mixed_non_finite_group_leaves_other_groups_unchanged(dim, chunk):
+    """A group whose seeds are NaN shares its warp's off-cell gather queue with valid
+    groups; every other group must come out exactly as without it."""
+    if dim == 2:
+        shape, pts, snaps, pos = _blend_case_2d(16, 8)
+        series = SnapshotSeries(GridSpec.from_points(pts, shape), snaps, precision="fx15")
+        kw = dict(integrator="rk4", time_mode="blend", h=0.013, num_steps=40, snapshot_dt=0.05)
+    else:
+        n, S = 24, 8
+        ax = flows.periodic_axis(n)
+        snaps = flows.abc_snapshots(ax, ax, ax, np.arange(S) * (2 * math.pi / S))
+        grid = GridSpec.from_points(flows.grid_points_3d(ax, ax, ax), (n, n, n), periodic=True)
+        series = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+        pos = flows.seeds_3d(np.random.default_rng(4).uniform(0, 2 * math.pi, (128, 3)), 1e-3)
+        kw = dict(integrator="rk4", time_mode="blend", h=0.02, num_steps=60,
+                  snapshot_dt=2 * math.pi / S)
+    if chunk:
+        kw.update(chunk_steps=chunk, sort_every=1)
+    K = 2 * dim
+    N = pos.shape[0] // K
+    bad = 5
+    rows = np.arange(K) * N + bad
+    p1 = torch.as_tensor(pos, device="cuda")
+    f1 = host(run_window(series, p1, **kw))
+    pos2 = pos.copy()
+    pos2[rows] = np.nan
+    p2 = torch.as_tensor(pos2, device="cuda")
+    f2 = host(run_window(series, p2, **kw))
+    keep = np.setdiff1d(np.arange(K * N), rows)
+    np.testing.assert_array_equal(host(p2)[keep], host(p1)[keep])
+    np.testing.assert_array_equal(np.delete(f2, bad), np.delete(f1, bad))
+
+
 def test_fx15_range_is_exact_and_repeatable_with_negative_zeros():
     """The FX15 value range (per-component min / max over the series) must not depend
     on the order of the device's atomic updates; exact -0.0 values (a velocity field
