@@ -457,7 +457,11 @@ def run_ours(args):
                        "chunk_steps": chunk, "sort_every": args.sort_every,
                        "particles": K * N, "groups": N, "rk4_steps": w["num_steps"],
                        "particle_steps_per_window": particle_steps,
-                       "l2": "inputs larger than L2 (positions 2.4 GB, packed snapshots)",
+                       # the mixed path also advects each group's centroid (overhead,
+                       # not counted in `value`): K+1 trajectories per group
+                       "trajectory_steps_per_window_with_centroids":
+                           particle_steps // K * (K + 1) if elem == 2 else particle_steps,
+                       "l2":"inputs larger than L2 (positions 2.4 GB, packed snapshots)",
                        "rank_windows": "rank r starts at t0 = r * snapshot_dt"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": args.steps * launches_per_window, "clocks": clk, "plain_fp64": plain,
