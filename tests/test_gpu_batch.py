@@ -120,3 +120,69 @@ def test_device_turbulence_snapshots_match_host():
     host = turb.snapshots(64, times)
     dev = turb.snapshots_device(64, times).cpu().numpy()
     np.testing.assert_allclose(dev, host, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("integrator,time_mode", [("euler", "blend"), ("ab2", "blend"),
+                                                  ("rk4", "hold"), ("ab2", "hold")])
+def test_batch_integrators_and_hold_equal_windows_alone(series, integrator, time_mode):
+    """The persistent kernel's Euler / AB2 paths and HOLD windows (step i holds snapshot
+    first_snapshot + i) give the bits of the same windows run one by one."""
+    rng = np.random.default_rng(7)
+    runs, alone = [], []
+    for i in range(5):
+        cents = rng.uniform(0, 2 * math.pi, (int(rng.integers(40, 2500)), 2))
+        pos = flows.seeds_2d(cents, 5e-4)
+        steps = int(rng.integers(4, 18))  # HOLD: first + steps stays inside the 40 snapshots
+        if time_mode == "hold":
+            h = DT if i % 2 else -DT
+            first = int(rng.integers(steps, S - steps))
+            t0 = 0.0
+        else:
+            h = 0.01 if i % 2 else -0.01
+            first = 0
+            span = steps * abs(h)
+            t0 = rng.uniform(span, (S - 1) * DT) if h < 0 else rng.uniform(0, (S - 1) * DT - span)
+        mp = 0.37 + 0.01 * i  # explicit: both routes then normalise by the same T
+        pt = torch.as_tensor(pos, device="cuda")
+        f = run_window(series, pt, integrator=integrator, time_mode=time_mode, h=h,
+                       num_steps=steps, t0=t0, first_snapshot=first, map_period=mp,
+                       snapshot_dt=DT)
+        torch.cuda.synchronize()
+        alone.append((pt.cpu().numpy(), f.cpu().numpy()))
+        runs.append(WindowSpecRun(torch.as_tensor(pos, device="cuda"), t0, h, steps,
+                                  map_period=mp, first_snapshot=first))
+    batch = WindowBatch(series, runs, integrator=integrator, time_mode=time_mode,
+                        snapshot_dt=DT)
+    ftles = batch.run(Schedule(4, 1))
+    torch.cuda.synchronize()
+    for (rp, rf), run, f in zip(alone, runs, ftles):
+        np.testing.assert_array_equal(run.positions.cpu().numpy(), rp)
+        np.testing.assert_array_equal(f.cpu().numpy(), rf)
+
+
+@pytest.mark.parametrize("integrator", ["rk4", "ab2"])
+def test_batch_3d_periodic_equals_windows_alone(integrator):
+    n, S3 = 24, 8
+    dt = 2 * math.pi / S3
+    ax = flows.periodic_axis(n)
+    snaps = flows.abc_snapshots(ax, ax, ax, np.arange(S3) * dt)
+    grid = GridSpec.from_points(flows.grid_points_3d(ax, ax, ax), (n, n, n), periodic=True)
+    s3 = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+    rng = np.random.default_rng(9)
+    runs, alone = [], []
+    for i in range(4):
+        pos = flows.seeds_3d(rng.uniform(0, 2 * math.pi, (int(rng.integers(30, 900)), 3)), 1e-3)
+        h = 0.02 if i % 2 else -0.02
+        steps = int(rng.integers(10, 70))
+        t0 = rng.uniform(0, 10.0)  # the series is periodic in time
+        pt = torch.as_tensor(pos, device="cuda")
+        f = run_window(s3, pt, integrator=integrator, time_mode="blend", h=h, num_steps=steps,
+                       t0=t0, snapshot_dt=dt)
+        torch.cuda.synchronize()
+        alone.append((pt.cpu().numpy(), f.cpu().numpy()))
+        runs.append(WindowSpecRun(torch.as_tensor(pos, device="cuda"), t0, h, steps))
+    ftles = WindowBatch(s3, runs, integrator=integrator, snapshot_dt=dt).run(Schedule(2, 0))
+    torch.cuda.synchronize()
+    for (rp, rf), run, f in zip(alone, runs, ftles):
+        np.testing.assert_array_equal(run.positions.cpu().numpy(), rp)
+        np.testing.assert_array_equal(f.cpu().numpy(), rf)
