@@ -9,13 +9,20 @@ take work items (128 groups of one window) from a counter, longest windows first
 
 ``WindowBatch`` builds the plan once (``ftle_windows_plan``), keeps it on the
 device, and runs it directly or as a captured CUDA graph (``capture()`` /
-``replay()``).  ``autotune()`` times the schedule candidates (CTAs per SM,
+``replay()``).  A persistent work item keeps its 128 groups for the whole window (the
+single-window path re-sorts between chunks instead), so by default the batch hands the
+kernel each seed buffer in Morton order of the groups' initial centroids: a work item
+then holds a compact patch of the domain and its gathers share cache lines.  Each run
+gathers the seeds into that order, runs the kernel, and scatters FTLE (and the final
+positions of windows that update them) back to the caller's order; per-group results
+are the same bits in either order.  ``autotune()`` times the schedule candidates (CTAs per SM,
 ordering) on the batch itself and keeps the fastest; results are cached per
 batch shape in ``~/.cache/pyftle_b200/tuning.json``.
 """
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import json
 import os
@@ -52,24 +59,81 @@ class Schedule:
     order: int = 1  # 1: longest windows first, 0: as given
 
 
+def _spread_bits(x: torch.Tensor, bits: int, dim: int) -> torch.Tensor:
+    r = torch.zeros_like(x)
+    for b in range(bits):
+        r |= ((x >> b) & 1) << (dim * b)
+    return r
+
+
+def morton_order(positions: torch.Tensor, grid) -> torch.Tensor:
+    """Permutation of a role-blocked (K*N, dim) seed buffer's N groups that sorts them by
+    the Morton code of their centroid's cell on a 2^bits-per-axis coarse grid (2D 10
+    bits, 3D 7).  Non-finite centroids sort to the grid's far corner."""
+    dim = grid.dim
+    K = 2 * dim
+    n = positions.shape[0] // K
+    cent = positions.view(K, n, dim).mean(dim=0)
+    bits = 10 if dim == 2 else 7
+    key = torch.zeros(n, dtype=torch.int64, device=positions.device)
+    for a in range(dim):
+        extent = grid.spacing[a] * (grid.shape[a] if grid.periodic else max(grid.shape[a] - 1, 1))
+        f = (cent[:, a] - grid.origin[a]) / extent
+        if grid.periodic:
+            f = f - torch.floor(f)
+        f = torch.nan_to_num(f, nan=1.0, posinf=1.0, neginf=0.0)
+        cell = (f * (1 << bits)).clamp(0, (1 << bits) - 1).to(torch.int64)
+        key |= _spread_bits(cell, bits, dim) << a
+    return torch.argsort(key, stable=True)
+
+
 class WindowBatch:
     def __init__(self, series: SnapshotSeries, windows: Sequence[WindowSpecRun], *,
                  integrator: str = "rk4", time_mode: str = "blend",
                  snapshot_t0: float = 0.0, snapshot_dt: float = 1.0,
-                 schedule: Schedule = Schedule()):
+                 schedule: Schedule = Schedule(), spatial_order: bool = True):
         if series.storage == _lib.F64:
             raise ValueError("batched windows run on the mixed-precision path (fx15/fp16/bf16)")
         self.series = series
         self.windows = list(windows)
         self.kw = dict(integrator=integrator, time_mode=time_mode, snapshot_t0=snapshot_t0,
                        snapshot_dt=snapshot_dt)
-        arr = (_lib.FtleWindow * len(self.windows))()
-        for i, w in enumerate(self.windows):
-            n = w.positions.shape[0] // (2 * series.grid.dim)
+        dim = series.grid.dim
+        K = 2 * dim
+        # Spatial order: one permuted copy per distinct seed buffer (windows sharing
+        # read-only seeds share it), one FTLE buffer per window in that order.
+        self.spatial_order = bool(spatial_order)
+        self._src: List[torch.Tensor] = []      # caller's seed buffers
+        self._perm: List[torch.Tensor] = []     # group permutation per buffer
+        self._sorted: List[torch.Tensor] = []   # seeds in Morton order
+        self._shared: List[bool] = []          # buffer is read-only seeds (shareable)
+        self._win_src: List[int] = []
+        self._win_ftle: List[torch.Tensor] = []
+        for w in self.windows:
+            n = w.positions.shape[0] // K
             if w.ftle is None:
                 w.ftle = torch.empty(n, dtype=torch.float64, device=w.positions.device)
+            if not self.spatial_order:
+                continue
+            k = next((i for i, t in enumerate(self._src)
+                      if w.keep_positions and self._shared[i]
+                      and t.data_ptr() == w.positions.data_ptr()), None)
+            if k is None:
+                self._src.append(w.positions)
+                self._shared.append(bool(w.keep_positions))
+                perm = morton_order(w.positions, series.grid)
+                self._perm.append(perm)
+                self._sorted.append(torch.empty_like(w.positions))
+                k = len(self._src) - 1
+            self._win_src.append(k)
+            self._win_ftle.append(torch.empty_like(w.ftle))
+        self._gather()
+        arr = (_lib.FtleWindow * len(self.windows))()
+        for i, w in enumerate(self.windows):
+            pos = self._sorted[self._win_src[i]] if self.spatial_order else w.positions
+            ftle = self._win_ftle[i] if self.spatial_order else w.ftle
             mp = w.map_period if w.map_period is not None else w.num_steps * abs(w.h)
-            arr[i] = window_descriptor(series, w.positions, w.ftle, h=w.h, num_steps=w.num_steps,
+            arr[i] = window_descriptor(series, pos, ftle, h=w.h, num_steps=w.num_steps,
                                        map_period=mp, t0=w.t0, first_snapshot=w.first_snapshot,
                                        keep_positions=w.keep_positions, **self.kw)
         self.desc = arr
@@ -93,11 +157,34 @@ class WindowBatch:
         self._plans[order] = dev
         return dev
 
+    def _view(self, t: torch.Tensor) -> torch.Tensor:
+        K = 2 * self.series.grid.dim
+        return t.view(K, t.shape[0] // K, self.series.grid.dim)
+
+    def _gather(self) -> None:
+        """Seeds (caller's order) -> Morton-ordered copies."""
+        for src, perm, dst in zip(self._src, self._perm, self._sorted):
+            torch.index_select(self._view(src), 1, perm, out=self._view(dst))
+
+    def _scatter(self) -> None:
+        """FTLE, and the final positions of windows that update them, back to the
+        caller's order."""
+        for i, w in enumerate(self.windows):
+            k = self._win_src[i]
+            w.ftle.index_copy_(0, self._perm[k], self._win_ftle[i])
+            if not w.keep_positions:
+                self._view(w.positions).index_copy_(1, self._perm[k], self._view(self._sorted[k]))
+
     def run(self, schedule: Optional[Schedule] = None, stream=None) -> List[torch.Tensor]:
         sch = schedule or self.schedule
         plan = self._plan(sch.order)
-        _lib.call("ftle_windows_run_mixed", self.desc, self.count, plan.data_ptr(), plan.numel(),
-                  int(sch.ctas_per_sm), stream_ptr(stream))
+        with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+            if self.spatial_order:
+                self._gather()
+            _lib.call("ftle_windows_run_mixed", self.desc, self.count, plan.data_ptr(),
+                      plan.numel(), int(sch.ctas_per_sm), stream_ptr(stream))
+            if self.spatial_order:
+                self._scatter()
         return [w.ftle for w in self.windows]
 
     @property

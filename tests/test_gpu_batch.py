@@ -186,3 +186,28 @@ def test_batch_3d_periodic_equals_windows_alone(integrator):
     for (rp, rf), run, f in zip(alone, runs, ftles):
         np.testing.assert_array_equal(run.positions.cpu().numpy(), rp)
         np.testing.assert_array_equal(f.cpu().numpy(), rf)
+
+
+def test_batch_spatial_order_is_bit_identical(series):
+    """Morton-ordered groups (the default) and the caller's order give the same bits,
+    for windows that update their positions and windows sharing read-only seeds."""
+    rng = np.random.default_rng(12)
+    shared = torch.as_tensor(flows.seeds_2d(rng.uniform(0, 2 * math.pi, (1500, 2)), 5e-4),
+                             device="cuda")
+    own = [flows.seeds_2d(rng.uniform(0, 2 * math.pi, (int(rng.integers(50, 900)), 2)), 5e-4)
+           for _ in range(3)]
+    out = []
+    for order in (False, True):
+        runs = [WindowSpecRun(shared, 0.3 + 0.2 * i, 0.01, 20 + 7 * i, keep_positions=True)
+                for i in range(3)]
+        runs += [WindowSpecRun(torch.as_tensor(p, device="cuda"), 0.5, -0.01, 25) for p in own]
+        f = WindowBatch(series, runs, snapshot_dt=DT, spatial_order=order).run(Schedule(4, 1))
+        torch.cuda.synchronize()
+        out.append(([x.cpu().numpy() for x in f], [r.positions.cpu().numpy() for r in runs[3:]]))
+    for a, b in zip(out[0][0], out[1][0]):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(shared.cpu().numpy()[:4],
+                                  flows.seeds_2d(np.random.default_rng(12).uniform(
+                                      0, 2 * math.pi, (1500, 2)), 5e-4)[:4])
