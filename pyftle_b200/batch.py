@@ -110,6 +110,11 @@ class WindowBatch:
         self._win_src: List[int] = []
         self._win_ftle: List[torch.Tensor] = []
         for w in self.windows:
+            p = w.positions
+            if (p.dtype != torch.float64 or not p.is_cuda or not p.is_contiguous()
+                    or p.ndim != 2 or p.shape[1] != dim or p.shape[0] % K):
+                raise ValueError(f"positions must be a contiguous float64 CUDA tensor of shape "
+                                 f"({K}*N, {dim})")
             n = w.positions.shape[0] // K
             if w.ftle is None:
                 w.ftle = torch.empty(n, dtype=torch.float64, device=w.positions.device)
