@@ -523,12 +523,15 @@ def run_batched(args):
     for _ in range(args.warmup):
         batch.replay()
     torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")), enabled=not args.no_clocks)
+    clocks.start()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
     for _ in range(args.steps):
         batch.replay()
     b.record()
     torch.cuda.synchronize()
+    clk = clocks.stop()
     ms = a.elapsed_time(b) / args.steps
     ps = batch.particle_steps
     value = ps / (ms / 1e3)
@@ -571,7 +574,7 @@ def run_batched(args):
                        "speedup_chosen_vs_plain": value / plain,
                        "ftle_rel_err_l2_per_window": errs,
                        "ftle_mean_max_T_per_window": ftle_stats},
-        "gpu_launches": args.steps * 1,
+        "gpu_launches": args.steps * 1, "clocks": clk,
     }
     print(json.dumps(line), flush=True)
     return 0
