@@ -225,10 +225,14 @@ int ftle_windows_run_mixed(const ftle_window *windows, int32_t count, void *devi
  * array built into the library, reserved on every GPU that loads it until
  * the process exits.  No counterpart in the reference.  Windows needing more
  * than 32 MiB (ftle_window_workspace_bytes) are rejected with
- * FTLE_ERR_INVALID.  The first call on a device looks up the array's device
- * address, so make it before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (other streams, other threads) race
- * and must be serialised by the caller. */
+ * FTLE_ERR_INVALID.  The first call on a device (and again after the device's
+ * context was reset) looks up the array's device address; under CUDA's
+ * default lazy module loading that first call is also where the 32 MiB is
+ * reserved, and where it fails with FTLE_ERR_CUDA if the device has no room
+ * left.  Make that first call before any stream capture.  All calls share the
+ * one array, which keeps the last call's contents: calls that overlap on the
+ * GPU (other streams, other threads) race and must be serialised by the
+ * caller. */
 int ftle_window_run_mixed_chunked_static(const ftle_window *w, int32_t chunk_steps,
                                          int32_t sort_every, void *stream);
 
@@ -305,6 +309,22 @@ int ftle_surrogate_pack(const void *w0, const void *w1, const void *w2, const vo
 int ftle_surrogate_ftle(const double *points, int64_t n, double t0, const void *packed,
                         const float *bias, const float *freq, double out_scale, double T,
                         double *ftle, double *end_positions, int32_t *error_word, void *stream);
+
+/* ---- measurement -----------------------------------------------------------
+ * Gather-rate probe for the roofline of the window kernels (no counterpart in
+ * the reference).  `blocks` blocks of 128 threads each issue iters x 8
+ * independent 16-byte read-only loads (ftle_gather_probe_loads() in total) at
+ * pseudo-random records of a region of `region_bytes` (a power of two, at most
+ * 512 MiB and buf_bytes): one region per block when per_block_region != 0
+ * (a few KB: L1-resident), else one region shared by all blocks (~32 MB:
+ * L2-resident).  The lanes of a warp load within a random window of
+ * lane_span_bytes (power of two: 16 .. region_bytes).  buf: 16-byte aligned,
+ * zero-filled; sink: one device uint32 (written only if the loads XOR to a
+ * magic word, never for zeros).  Time it with events on `stream`. */
+int ftle_gather_probe(const void *buf, int64_t buf_bytes, int64_t region_bytes,
+                      int64_t lane_span_bytes, int32_t per_block_region, int32_t blocks,
+                      int32_t iters, uint32_t seed, void *sink, void *stream);
+int64_t ftle_gather_probe_loads(int32_t blocks, int32_t iters);
 
 #ifdef __cplusplus
 }

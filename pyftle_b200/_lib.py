@@ -77,6 +77,9 @@ SIGNATURES = {
     "ftle_packed_snapshot_bytes": (ctypes.c_int64, [_i32, _i64, _i32, _i32]),
     "ftle_pack_snapshots": (ctypes.c_int, [_i32, _i64, _i32, _i32, _c_dp, _i32, _c_dp, _c_dp]),
     "ftle_window_run_f64": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp]),
+    "ftle_gather_probe": (ctypes.c_int, [_c_dp, _i64, _i64, _i64, _i32, _i32, _i32,
+                                         ctypes.c_uint32, _c_dp, _c_dp]),
+    "ftle_gather_probe_loads": (_i64, [_i32, _i32]),
     "ftle_window_run_mixed": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp]),
     "ftle_window_workspace_bytes": (ctypes.c_int64, [ctypes.POINTER(FtleWindow)]),
     "ftle_window_run_mixed_chunked": (ctypes.c_int, [ctypes.POINTER(FtleWindow), _c_dp, _i64,

@@ -118,11 +118,17 @@ class WindowBatch:
             n = w.positions.shape[0] // K
             if w.ftle is None:
                 w.ftle = torch.empty(n, dtype=torch.float64, device=w.positions.device)
+            elif (w.ftle.dtype != torch.float64 or w.ftle.device != p.device
+                  or not w.ftle.is_contiguous() or w.ftle.numel() != n):
+                raise ValueError(f"ftle must be a contiguous float64 tensor of {n} elements "
+                                 f"on {p.device}")
             if not self.spatial_order:
                 continue
+            # read-only seeds are shared only with a window over the very same buffer
+            # (same start and shape; a prefix view of a larger buffer is not the same)
             k = next((i for i, t in enumerate(self._src)
                       if w.keep_positions and self._shared[i]
-                      and t.data_ptr() == w.positions.data_ptr()), None)
+                      and t.data_ptr() == p.data_ptr() and t.shape == p.shape), None)
             if k is None:
                 self._src.append(w.positions)
                 self._shared.append(bool(w.keep_positions))
@@ -137,7 +143,12 @@ class WindowBatch:
         for i, w in enumerate(self.windows):
             pos = self._sorted[self._win_src[i]] if self.spatial_order else w.positions
             ftle = self._win_ftle[i] if self.spatial_order else w.ftle
-            mp = w.map_period if w.map_period is not None else w.num_steps * abs(w.h)
+            if w.map_period is not None:
+                mp = w.map_period
+            elif time_mode == "hold":  # the reference's T = (p - 1)|dt| (ftle_solver.py:156)
+                mp = (w.num_steps - 1) * abs(w.h)
+            else:
+                mp = w.num_steps * abs(w.h)
             arr[i] = window_descriptor(series, pos, ftle, h=w.h, num_steps=w.num_steps,
                                        map_period=mp, t0=w.t0, first_snapshot=w.first_snapshot,
                                        keep_positions=w.keep_positions, **self.kw)

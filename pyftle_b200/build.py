@@ -34,6 +34,7 @@ SOURCES = {
     "no_alloc.cu": [],
     "mlp.cu": [],
     "mlp_fused.cu": [],
+    "probe.cu": [],
 }
 HEADERS = ["common.cuh", "umma.cuh"]
 

@@ -81,6 +81,14 @@ def window_descriptor(series: SnapshotSeries, positions: torch.Tensor, ftle: Opt
         raise ValueError("positions must be a contiguous float64 CUDA tensor")
     if positions.ndim != 2 or positions.shape[1] != dim or positions.shape[0] % K:
         raise ValueError(f"positions must have shape ({K}*N, {dim})")
+    n = positions.shape[0] // K
+    if ftle is not None:
+        # the kernels write N float64 values through the raw pointer: anything else
+        # would be written out of bounds or misread
+        if (ftle.dtype != torch.float64 or ftle.device != positions.device
+                or not ftle.is_contiguous() or ftle.numel() != n):
+            raise ValueError(f"ftle must be a contiguous float64 tensor of {n} elements on "
+                             f"{positions.device}")
     w = _lib.FtleWindow()
     w.grid = series.grid.to_abi()
     w.snapshots = series.packed.data_ptr()
@@ -97,7 +105,7 @@ def window_descriptor(series: SnapshotSeries, positions: torch.Tensor, ftle: Opt
     w.num_steps = int(num_steps)
     w.flags = _lib.KEEP_POSITIONS if keep_positions else 0
     w.positions = positions.data_ptr()
-    w.num_groups = positions.shape[0] // K
+    w.num_groups = n
     w.map_period = float(map_period)
     w.ftle = 0 if ftle is None else ftle.data_ptr()
     return w

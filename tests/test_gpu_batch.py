@@ -211,3 +211,63 @@ def test_batch_spatial_order_is_bit_identical(series):
     np.testing.assert_array_equal(shared.cpu().numpy()[:4],
                                   flows.seeds_2d(np.random.default_rng(12).uniform(
                                       0, 2 * math.pi, (1500, 2)), 5e-4)[:4])
+
+
+def test_batch_hold_default_map_period_equals_window_alone(series):
+    """HOLD windows without an explicit map period are normalised like the reference
+    (T = (steps - 1)|h|, ftle_solver.py:156), in a batch as when run alone."""
+    rng = np.random.default_rng(21)
+    runs, alone = [], []
+    for i in range(3):
+        pos = flows.seeds_2d(rng.uniform(0, 2 * math.pi, (int(rng.integers(40, 700)), 2)), 5e-4)
+        steps = int(rng.integers(4, 15))
+        h = DT if i % 2 else -DT
+        first = int(rng.integers(steps, S - steps))
+        pt = torch.as_tensor(pos, device="cuda")
+        f = run_window(series, pt, integrator="rk4", time_mode="hold", h=h, num_steps=steps,
+                       first_snapshot=first, snapshot_dt=DT)
+        torch.cuda.synchronize()
+        alone.append(f.cpu().numpy())
+        runs.append(WindowSpecRun(torch.as_tensor(pos, device="cuda"), 0.0, h, steps,
+                                  first_snapshot=first))
+    ftles = WindowBatch(series, runs, time_mode="hold", snapshot_dt=DT).run(Schedule(4, 1))
+    torch.cuda.synchronize()
+    for rf, f in zip(alone, ftles):
+        np.testing.assert_array_equal(f.cpu().numpy(), rf)
+
+
+def test_batch_and_window_reject_bad_ftle_buffers(series):
+    pos = torch.as_tensor(flows.seeds_2d(np.full((10, 2), 1.0), 5e-4), device="cuda")
+    bad = [torch.empty(9, dtype=torch.float64, device="cuda"),
+           torch.empty(10, dtype=torch.float32, device="cuda"),
+           torch.empty(20, dtype=torch.float64, device="cuda")[::2],
+           torch.empty(10, dtype=torch.float64)]
+    for f in bad:
+        with pytest.raises(ValueError, match="ftle must be"):
+            run_window(series, pos.clone(), time_mode="blend", h=0.01, num_steps=3,
+                       snapshot_dt=DT, ftle_out=f)
+        with pytest.raises(ValueError, match="ftle must be"):
+            WindowBatch(series, [WindowSpecRun(pos.clone(), 0.0, 0.01, 3, ftle=f)],
+                        snapshot_dt=DT)
+
+
+def test_batch_prefix_view_of_shared_seeds_is_not_shared(series):
+    """A window over a prefix view of another window's read-only seeds starts at the same
+    address; it must get its own ordered copy (and its own N), not the larger one."""
+    rng = np.random.default_rng(31)
+    big_h = flows.seeds_2d(rng.uniform(0, 2 * math.pi, (900, 2)), 5e-4)
+    big = torch.as_tensor(big_h, device="cuda")
+    n_small = 300
+    prefix = big[:4 * n_small]  # same data_ptr, fewer rows (role blocks of its own)
+    runs = [WindowSpecRun(big, 0.3, 0.01, 12, keep_positions=True),
+            WindowSpecRun(prefix, 0.3, 0.01, 12, keep_positions=True)]
+    ftles = WindowBatch(series, runs, snapshot_dt=DT).run(Schedule(4, 1))
+    torch.cuda.synchronize()
+    ref_big = run_window(series, big.clone(), integrator="rk4", time_mode="blend", h=0.01,
+                         num_steps=12, t0=0.3, snapshot_dt=DT)
+    ref_prefix = run_window(series, prefix.clone(), integrator="rk4", time_mode="blend",
+                            h=0.01, num_steps=12, t0=0.3, snapshot_dt=DT)
+    torch.cuda.synchronize()
+    assert ftles[1].numel() == n_small
+    np.testing.assert_array_equal(ftles[0].cpu().numpy(), ref_big.cpu().numpy())
+    np.testing.assert_array_equal(ftles[1].cpu().numpy(), ref_prefix.cpu().numpy())
