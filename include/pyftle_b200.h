@@ -208,7 +208,8 @@ int ftle_analytic_window_run(const ftle_flow *flow, int32_t integrator, double t
  * one window) from a counter until all are done.  Replaces the reference's
  * one-process-per-window ParallelExecutor (parallel.py:171-271) for the hot
  * path.  Build the plan once on the host (ftle_windows_plan: window table plus
- * work list; order 1 = longest windows first, 0 = as given), copy it to a
+ * work list; order 1 = longest windows first, 2 = by the start of each window's
+ * time range, 0 = as given), copy it to a
  * 256-byte aligned device buffer, then run it any number of times; the plan
  * holds the windows' device pointers.  The run only issues a memset of the
  * plan's counter and one kernel on `stream` (ctas_per_sm x 148 persistent CTAs,

@@ -56,7 +56,7 @@ class WindowSpecRun:
 @dataclass(frozen=True)
 class Schedule:
     ctas_per_sm: int = 4  # the kernel fits 4 blocks of 128 threads per SM
-    order: int = 1  # 1: longest windows first, 0: as given
+    order: int = 1  # 1: longest windows first, 2: by start of the time range, 0: as given
 
 
 def _spread_bits(x: torch.Tensor, bits: int, dim: int) -> torch.Tensor:
@@ -253,7 +253,7 @@ class WindowBatch:
         # blocks per SM the kernel can keep resident: 4 in 3D, up to 8 in 2D
         ctas = (1, 2, 3, 4) if self.series.grid.dim == 3 else (2, 4, 6, 8)
         cands = list(candidates) if candidates else [Schedule(c, o) for c in ctas
-                                                     for o in (1, 0)]
+                                                     for o in (1, 2, 0)]
         timings = []
         for sch in cands:
             if prologue:

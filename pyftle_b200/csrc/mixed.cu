@@ -289,11 +289,39 @@ __device__ __forceinline__ int wrap_near(int q, int n) {
   return q;
 }
 
-// Time-blended corner values v[c][q] of the cell whose lower corner is `cell`
-// (q = x + 2y (+ 4z)); false if the cell is outside a non-periodic grid.
+// ---------------------------------------------------------------------------
+// packed FP32 (sm_100 FFMA2 / FADD2 / FMUL2): two lanes of one 64-bit register pair
+// per instruction, each lane rounded exactly like the scalar fmaf / add / mul, so
+// a pair computes the same bits as two scalar operations.  Pairs are the (u, v)
+// velocity components of a corner or polynomial, or the same component of two
+// neighbours of a group (neighbours 2p and 2p+1, which share the centroid's cell).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));  // a + (-b) rounds as a - b
+}
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) { return fma2(t, sub2(b, a), a); }
+
+__device__ __forceinline__ float vsub(float a, float b) { return a - b; }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return sub2(a, b); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return fma2(a, b, c); }
+
+// Time-blended corner values of one cell, corner q = x + 2y (+ 4z): (u, v) paired, w apart.
+template <int DIM>
+struct CellVals {
+  float2 uv[1 << DIM];
+  float w[DIM == 3 ? 8 : 1];
+};
+
+// Corner values of the cell whose lower corner is `cell`; false if the cell is
+// outside a non-periodic grid.
 template <int DIM, int STORAGE, bool BLEND>
 __device__ __forceinline__ bool cell_values(const MixK &m, const unsigned char *__restrict__ recs,
-                                            float alpha, const int *cell, float (*v)[1 << DIM]) {
+                                            float alpha, const int *cell, CellVals<DIM> &v) {
   const GridK &g = m.w.g;
   int base = 0, step[DIM];
 #pragma unroll
@@ -308,6 +336,7 @@ __device__ __forceinline__ bool cell_values(const MixK &m, const unsigned char *
     }
     base += lo * m.stride[a];
   }
+  const float2 a2 = bc2(alpha);
 #pragma unroll
   for (int q = 0; q < (1 << DIM); ++q) {
     int idx = base;
@@ -318,95 +347,105 @@ __device__ __forceinline__ bool cell_values(const MixK &m, const unsigned char *
     }
     if constexpr (DIM == 2) {
       const uint2 r = __ldg(reinterpret_cast<const uint2 *>(recs) + idx);
-      const float u0 = Dec<STORAGE>::lo(r.x), v0 = Dec<STORAGE>::hi(r.x);
+      const float2 f0 = make_float2(Dec<STORAGE>::lo(r.x), Dec<STORAGE>::hi(r.x));
       if constexpr (BLEND) {
-        v[0][q] = lerpf(u0, Dec<STORAGE>::lo(r.y), alpha);
-        v[1][q] = lerpf(v0, Dec<STORAGE>::hi(r.y), alpha);
+        v.uv[q] = lerp2(f0, make_float2(Dec<STORAGE>::lo(r.y), Dec<STORAGE>::hi(r.y)), a2);
       } else {
-        v[0][q] = u0;
-        v[1][q] = v0;
+        v.uv[q] = f0;
       }
     } else {
       const uint4 r = __ldg(reinterpret_cast<const uint4 *>(recs) + idx);
-      const float u0 = Dec<STORAGE>::lo(r.x), v0 = Dec<STORAGE>::hi(r.x);
+      const float2 f0 = make_float2(Dec<STORAGE>::lo(r.x), Dec<STORAGE>::hi(r.x));
       const float w0 = Dec<STORAGE>::lo(r.y);
       if constexpr (BLEND) {
-        v[0][q] = lerpf(u0, Dec<STORAGE>::lo(r.z), alpha);
-        v[1][q] = lerpf(v0, Dec<STORAGE>::hi(r.z), alpha);
-        v[2][q] = lerpf(w0, Dec<STORAGE>::lo(r.w), alpha);
+        v.uv[q] = lerp2(f0, make_float2(Dec<STORAGE>::lo(r.z), Dec<STORAGE>::hi(r.z)), a2);
+        v.w[q] = lerpf(w0, Dec<STORAGE>::lo(r.w), alpha);
       } else {
-        v[0][q] = u0;
-        v[1][q] = v0;
-        v[2][q] = w0;
+        v.uv[q] = f0;
+        v.w[q] = w0;
       }
     }
   }
   return true;
 }
 
-// multilinear interpolation by lerps (x, then y, then z)
+// multilinear interpolation by lerps (x, then y, then z) of the (u, v) pair
 template <int DIM>
-__device__ __forceinline__ float interp_lerp(const float *v, const float *f) {
-  const float x0 = lerpf(v[0], v[1], f[0]);
-  const float x1 = lerpf(v[2], v[3], f[0]);
-  const float y0 = lerpf(x0, x1, f[1]);
+__device__ __forceinline__ float2 interp_lerp_uv(const float2 *v, const float *f) {
+  const float2 f0 = bc2(f[0]), f1 = bc2(f[1]);
+  const float2 x0 = lerp2(v[0], v[1], f0);
+  const float2 x1 = lerp2(v[2], v[3], f0);
+  const float2 y0 = lerp2(x0, x1, f1);
   if constexpr (DIM == 2) {
     return y0;
   } else {
-    const float x2 = lerpf(v[4], v[5], f[0]);
-    const float x3 = lerpf(v[6], v[7], f[0]);
-    return lerpf(y0, lerpf(x2, x3, f[1]), f[2]);
+    const float2 x2 = lerp2(v[4], v[5], f0);
+    const float2 x3 = lerp2(v[6], v[7], f0);
+    return lerp2(y0, lerp2(x2, x3, f1), bc2(f[2]));
   }
 }
 
-// p(x) = a0 + a1 x + a2 y (+ a3 z) + a4 xy + a5 xz + a6 yz + a7 xyz  (2D: a0 a1 a2 a3=xy)
-template <int DIM>
-__device__ __forceinline__ void poly_setup(const float *v, float *A) {
+// ... and of a single component (w in 3D)
+__device__ __forceinline__ float interp_lerp3(const float *v, const float *f) {
+  const float x0 = lerpf(v[0], v[1], f[0]);
+  const float x1 = lerpf(v[2], v[3], f[0]);
+  const float y0 = lerpf(x0, x1, f[1]);
+  const float x2 = lerpf(v[4], v[5], f[0]);
+  const float x3 = lerpf(v[6], v[7], f[0]);
+  return lerpf(y0, lerpf(x2, x3, f[1]), f[2]);
+}
+
+// p(x) = a0 + a1 x + a2 y (+ a3 z) + a4 xy + a5 xz + a6 yz + a7 xyz  (2D: a0 a1 a2 a3=xy),
+// for one component (T = float) or the (u, v) pair (T = float2)
+template <int DIM, typename T>
+__device__ __forceinline__ void poly_setup(const T *v, T *A) {
   if constexpr (DIM == 2) {
     A[0] = v[0];
-    A[1] = v[1] - v[0];
-    A[2] = v[2] - v[0];
-    A[3] = (v[3] - v[2]) - (v[1] - v[0]);
+    A[1] = vsub(v[1], v[0]);
+    A[2] = vsub(v[2], v[0]);
+    A[3] = vsub(vsub(v[3], v[2]), vsub(v[1], v[0]));
   } else {
     A[0] = v[0];
-    A[1] = v[1] - v[0];
-    A[2] = v[2] - v[0];
-    A[3] = v[4] - v[0];
-    A[4] = (v[3] - v[1]) - A[2];
-    A[5] = (v[5] - v[1]) - A[3];
-    A[6] = (v[6] - v[2]) - A[3];
-    A[7] = ((v[7] - v[6]) - (v[5] - v[4])) - ((v[3] - v[2]) - (v[1] - v[0]));
+    A[1] = vsub(v[1], v[0]);
+    A[2] = vsub(v[2], v[0]);
+    A[3] = vsub(v[4], v[0]);
+    A[4] = vsub(vsub(v[3], v[1]), A[2]);
+    A[5] = vsub(vsub(v[5], v[1]), A[3]);
+    A[6] = vsub(vsub(v[6], v[2]), A[3]);
+    A[7] = vsub(vsub(vsub(v[7], v[6]), vsub(v[5], v[4])), vsub(vsub(v[3], v[2]), vsub(v[1], v[0])));
   }
 }
 
-template <int DIM>
-__device__ __forceinline__ float poly_eval(const float *A, const float *f) {
+// p(f), with f given per axis as T (a pair holds the same coordinate twice)
+template <int DIM, typename T>
+__device__ __forceinline__ T poly_eval(const T *A, const T *f) {
   if constexpr (DIM == 2) {
-    return fmaf(f[0], fmaf(f[1], A[3], A[1]), fmaf(f[1], A[2], A[0]));
+    return vfma(f[0], vfma(f[1], A[3], A[1]), vfma(f[1], A[2], A[0]));
   } else {
-    const float x = f[0], y = f[1], z = f[2];
-    const float t1 = fmaf(z, A[7], A[4]);
-    const float t3 = fmaf(z, A[5], fmaf(y, t1, A[1]));
-    const float t4 = fmaf(z, A[6], A[2]);
-    return fmaf(z, A[3], fmaf(y, t4, fmaf(x, t3, A[0])));
+    const T x = f[0], y = f[1], z = f[2];
+    const T t1 = vfma(z, A[7], A[4]);
+    const T t3 = vfma(z, A[5], vfma(y, t1, A[1]));
+    const T t4 = vfma(z, A[6], A[2]);
+    return vfma(z, A[3], vfma(y, t4, vfma(x, t3, A[0])));
   }
 }
 
-// p(f + d) - p(f), written so that no large terms cancel
+// p(f + d) - p(f) of one component for two neighbours at once (F = f + d), written
+// so that no large terms cancel.  `g` is the part that depends on the centroid's f
+// only: 3D gz = x (a7 y + a5) + a6 y + a3, 2D gy = a3 x + a2.
+//   3D: dx (a1 + a4 Y + a5 Z + a7 Y Z) + dy (a2 + a4 x + a6 Z + a7 x Z) + dz gz
+//   2D: dx (a1 + a3 Y) + dy gy
 template <int DIM>
-__device__ __forceinline__ float poly_diff(const float *A, const float *f, const float *d,
-                                           const float *F) {  // F = f + d
+__device__ __forceinline__ float2 poly_diff_pair(const float *A, float x, float g, const float2 *F,
+                                                 const float2 *d) {
   if constexpr (DIM == 2) {
-    // a1 dx + a2 dy + a3 (dx Y' + x dy)
-    return fmaf(d[0], fmaf(A[3], F[1], A[1]), d[1] * fmaf(A[3], f[0], A[2]));
+    return fma2(d[0], fma2(bc2(A[3]), F[1], bc2(A[1])), mul2(d[1], bc2(g)));
   } else {
-    const float x = f[0], y = f[1];
-    const float Y = F[1], Z = F[2];
-    const float t = fmaf(A[7], Z, A[4]);
-    const float gx = fmaf(Y, t, fmaf(A[5], Z, A[1]));
-    const float gy = fmaf(x, t, fmaf(A[6], Z, A[2]));
-    const float gz = fmaf(x, fmaf(A[7], y, A[5]), fmaf(A[6], y, A[3]));
-    return fmaf(d[0], gx, fmaf(d[1], gy, d[2] * gz));
+    const float2 Y = F[1], Z = F[2];
+    const float2 t = fma2(bc2(A[7]), Z, bc2(A[4]));
+    const float2 gx = fma2(Y, t, fma2(bc2(A[5]), Z, bc2(A[1])));
+    const float2 gy = fma2(bc2(x), t, fma2(bc2(A[6]), Z, bc2(A[2])));
+    return fma2(d[0], gx, fma2(d[1], gy, mul2(d[2], bc2(g))));
   }
 }
 
@@ -469,15 +508,17 @@ struct WarpQueue {
   int ci[DIM][32];  // centroid cell of each lane's group
 };
 
-// Per stage: centroid velocity uc and, in place of the previous stage's kd[k], the
-// differences kd[k] = u(c + d_k + a*kd_k) - uc.
-// Neighbours inside the centroid's cell use the cell polynomial; the others are
-// queued per warp and gathered 32 at a time, so no lane idles in a divergent loop.
+// Per stage: centroid velocity uc and, in place of the previous stage's kd, the
+// differences kd[p][a] = u(c + d_k + as*kd_k) - uc for the neighbour pair
+// k = 2p, 2p+1 (lanes .x, .y).  Neighbours inside the centroid's cell use the
+// cell polynomial; the others are queued per warp and gathered 32 at a time, so
+// no lane idles in a divergent loop.  `dpl`: this thread's offsets in shared
+// memory, float2 planes (neighbour pair p, axis a) at stride kBlock.
 template <int DIM, int STORAGE, bool BLEND>
 __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
                                            const unsigned char *__restrict__ recs, float alpha,
-                                           const double *cs, const float *d,
-                                           float (*kd)[DIM], float as, float *uc,
+                                           const double *cs, const float2 *dpl,
+                                           float2 (*kd)[DIM], float as, float *uc,
                                            float *slots_base, WarpQueue<DIM> &wq, int lane) {
   constexpr int K = 2 * DIM;
   constexpr int NC = 1 << DIM;
@@ -494,48 +535,90 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
     ci[a] = ok ? (int)fl : 0;
     fc[a] = ok ? (float)(p - fl) : 0.0f;
   }
-  float A[DIM][NC];
+  float2 fcb[DIM];
+#pragma unroll
+  for (int a = 0; a < DIM; ++a) fcb[a] = bc2(fc[a]);
+  // the centroid cell's polynomial: (u, v) paired, w apart
+  float2 Auv[NC];
+  float Aw[NC];  // w (3D only)
   bool cin;
   {
-    float v[DIM][NC];
+    CellVals<DIM> v;
     cin = ok && cell_values<DIM, STORAGE, BLEND>(m, recs, alpha, ci, v);
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) poly_setup<DIM>(v[c], A[c]);
+    poly_setup<DIM>(v.uv, Auv);
+    if constexpr (DIM == 3) poly_setup<DIM>(v.w, Aw);
   }
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    const float p = poly_eval<DIM>(A[c], fc);
-    uc[c] = cin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
+  {
+    float2 puv = poly_eval<DIM>(Auv, fcb);
+    if constexpr (FX)
+      puv = fma2(make_float2(hd.scale[0], hd.scale[1]), puv,
+                 make_float2(hd.offset[0], hd.offset[1]));
+    uc[0] = cin ? puv.x : 0.0f;
+    uc[1] = cin ? puv.y : 0.0f;
+    if constexpr (DIM == 3) {
+      const float pw = poly_eval<DIM>(Aw, fc);
+      uc[2] = cin ? (FX ? fmaf(hd.scale[2], pw, hd.offset[2]) : pw) : 0.0f;
+    }
   }
-  // pass 1: every neighbour through the cell polynomial; flag those outside the cell
+  // the part of p(f + d) - p(f) that depends on the centroid only, per component
+  float g[DIM];
+  if constexpr (DIM == 2) {
+    const float2 gp = fma2(Auv[3], fcb[0], Auv[2]);
+    g[0] = gp.x;
+    g[1] = gp.y;
+  } else {
+    const float2 gp = fma2(fcb[0], fma2(Auv[7], fcb[1], Auv[5]), fma2(Auv[6], fcb[1], Auv[3]));
+    g[0] = gp.x;
+    g[1] = gp.y;
+    g[2] = fmaf(fc[0], fmaf(Aw[7], fc[1], Aw[5]), fmaf(Aw[6], fc[1], Aw[3]));
+  }
+  // pass 1: every neighbour through the cell polynomial, two at a time; flag those
+  // outside the cell
   unsigned off = 0;
+  const float2 as2 = bc2(as);
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    float dl[DIM], F[DIM];
-    bool same = true;
+  for (int p = 0; p < DIM; ++p) {
+    float2 dl[DIM], F[DIM];
+    bool same0 = true, same1 = true;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
       // explicit roundings: the cell test and the polynomial use the same F and dl
-      // whatever the compiler schedules (no contraction into one FMA)
-      dl[a] = __fmul_rn(fmaf(as, kd[k][a], d[(k * DIM + a) * kBlock]), m.inv_spf[a]);
-      F[a] = __fadd_rn(fc[a], dl[a]);
-      same = same && F[a] >= 0.0f && F[a] < 1.0f;
+      dl[a] = mul2(fma2(as2, kd[p][a], dpl[(p * DIM + a) * kBlock]), bc2(m.inv_spf[a]));
+      F[a] = add2(fcb[a], dl[a]);
+      same0 = same0 && F[a].x >= 0.0f && F[a].x < 1.0f;
+      same1 = same1 && F[a].y >= 0.0f && F[a].y < 1.0f;
     }
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-      const float dp = poly_diff<DIM>(A[c], fc, dl, F);
-      kd[k][c] = cin ? (FX ? hd.scale[c] * dp : dp) : 0.0f;
+      float Ac[NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i) Ac[i] = c == 0 ? Auv[i].x : (c == 1 ? Auv[i].y : Aw[i]);
+      float2 dp = poly_diff_pair<DIM>(Ac, fc[0], g[c], F, dl);
+      if constexpr (FX) dp = mul2(bc2(hd.scale[c]), dp);
+      kd[p][c] = make_float2(cin ? dp.x : 0.0f, cin ? dp.y : 0.0f);
     }
+    const int k0 = 2 * p, k1 = 2 * p + 1;
     // 2D stores every neighbour's F without a branch (most warps have an off-cell
     // neighbour in most stages); 3D stores only the off-cell ones (measured faster)
     if constexpr (DIM == 2) {
-      off |= (!same && ok) ? 1u << k : 0u;
+      off |= (!same0 && ok) ? 1u << k0 : 0u;
+      off |= (!same1 && ok) ? 1u << k1 : 0u;
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
-    } else if (!same && ok) {
-      off |= 1u << k;
+      for (int a = 0; a < DIM; ++a) {
+        slots[(k0 * DIM + a) * kBlock] = F[a].x;
+        slots[(k1 * DIM + a) * kBlock] = F[a].y;
+      }
+    } else {
+      if (!same0 && ok) {
+        off |= 1u << k0;
 #pragma unroll
-      for (int a = 0; a < DIM; ++a) slots[(k * DIM + a) * kBlock] = F[a];
+        for (int a = 0; a < DIM; ++a) slots[(k0 * DIM + a) * kBlock] = F[a].x;
+      }
+      if (!same1 && ok) {
+        off |= 1u << k1;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) slots[(k1 * DIM + a) * kBlock] = F[a].y;
+      }
     }
   }
   if constexpr (DIM == 2) {
@@ -576,12 +659,17 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
         cell[a] = wq.ci[a][owner] + (int)fo;
         q[a] = F - fo;
       }
-      float v[DIM][NC];
+      CellVals<DIM> v;
       const bool kin = cell_values<DIM, STORAGE, BLEND>(m, recs, alpha, cell, v);
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        const float p = interp_lerp<DIM>(v[c], q);
-        slots_base[dst + c * kBlock] = kin ? (FX ? fmaf(hd.scale[c], p, hd.offset[c]) : p) : 0.0f;
+      float2 puv = interp_lerp_uv<DIM>(v.uv, q);
+      if constexpr (FX)
+        puv = fma2(make_float2(hd.scale[0], hd.scale[1]), puv,
+                   make_float2(hd.offset[0], hd.offset[1]));
+      slots_base[dst] = kin ? puv.x : 0.0f;
+      slots_base[dst + kBlock] = kin ? puv.y : 0.0f;
+      if constexpr (DIM == 3) {
+        const float pw = interp_lerp3(v.w, q);
+        slots_base[dst + 2 * kBlock] = kin ? (FX ? fmaf(hd.scale[2], pw, hd.offset[2]) : pw) : 0.0f;
       }
     }
   }
@@ -592,11 +680,15 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
 #pragma unroll
       for (int c = 0; c < DIM; ++c) {
         const float sv = slots[(k * DIM + c) * kBlock] - uc[c];
-        kd[k][c] = (off & (1u << k)) ? sv : kd[k][c];
+        float &r = (k & 1) ? kd[k >> 1][c].y : kd[k >> 1][c].x;
+        r = (off & (1u << k)) ? sv : r;
       }
     } else if (off & (1u << k)) {
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) kd[k][c] = slots[(k * DIM + c) * kBlock] - uc[c];
+      for (int c = 0; c < DIM; ++c) {
+        float &r = (k & 1) ? kd[k >> 1][c].y : kd[k >> 1][c].x;
+        r = slots[(k * DIM + c) * kBlock] - uc[c];
+      }
     }
   }
 }
@@ -653,30 +745,33 @@ __device__ __forceinline__ void group_from_positions(const MixK &m, const WinVar
   }
 }
 
-// Advect one group through steps [i0, i1) of the window.
+// Advect one group through steps [i0, i1) of the window.  The neighbour offsets
+// (dpl) and the RK4 accumulators (accp) live in this thread's shared-memory
+// columns as float2 planes (neighbour pair p = k/2, axis a) at stride kBlock.
 template <int DIM, int MODE, int INTEG, int STORAGE>
 __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, const Header16 &hd,
                                              GroupState<DIM> &st, int i0, int i1,
-                                             float *smem_slots, float *acc, float *dsm,
+                                             float *smem_slots, float2 *accp, float2 *dpl,
                                              WarpQueue<DIM> &wq, int lane) {
-  constexpr int K = 2 * DIM;
   constexpr bool BLEND = MODE == FTLE_BLEND;
   const bool periodic = m.w.g.periodic != 0;
   const double h = v.h;
   const float hf = (float)h;
-  float kc[DIM], kd[K][DIM], accc[DIM];
+  float kc[DIM], accc[DIM];
+  float2 kd[DIM][DIM];  // [pair][axis]
 #pragma unroll
   for (int a = 0; a < DIM; ++a) kc[a] = 0.0f;
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+  for (int p = 0; p < DIM; ++p)
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) kd[k][a] = 0.0f;
-  // the offsets live in this thread's shared-memory column during the step loop,
-  // which frees 3*K registers (the kernel then fits 4 blocks per SM)
+    for (int a = 0; a < DIM; ++a) kd[p][a] = make_float2(0.0f, 0.0f);
+  // the offsets live in shared memory during the step loop, which frees 3*K
+  // registers (the kernel then fits 4 blocks per SM)
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+  for (int p = 0; p < DIM; ++p)
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) dsm[(k * DIM + a) * kBlock] = st.d[k][a];
+    for (int a = 0; a < DIM; ++a)
+      dpl[(p * DIM + a) * kBlock] = make_float2(st.d[2 * p][a], st.d[2 * p + 1][a]);
 
   constexpr int NST = INTEG == FTLE_RK4 ? 4 : 1;
   for (int i = i0; i < i1; ++i) {
@@ -694,7 +789,7 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
 #pragma unroll
       for (int a = 0; a < DIM; ++a) cs[a] = fma((double)tc * h, (double)kc[a], st.c[a]);
       float uc[DIM];
-      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, dsm, kd, as, uc, smem_slots, wq,
+      eval_group<DIM, STORAGE, BLEND>(m, hd, recs, alpha, cs, dpl, kd, as, uc, smem_slots, wq,
                                       lane);
 #pragma unroll
       for (int a = 0; a < DIM; ++a) {
@@ -702,60 +797,71 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
         accc[a] = s == 0 ? uc[a] : fmaf(ws, uc[a], accc[a]);
       }
       if constexpr (INTEG == FTLE_RK4) {
+        const float2 ws2 = bc2(ws);
 #pragma unroll
-        for (int k = 0; k < K; ++k)
+        for (int p = 0; p < DIM; ++p)
 #pragma unroll
           for (int a = 0; a < DIM; ++a) {
-            float &r = acc[(k * DIM + a) * kBlock];
-            r = s == 0 ? kd[k][a] : fmaf(ws, kd[k][a], r);
+            float2 &r = accp[(p * DIM + a) * kBlock];
+            r = s == 0 ? kd[p][a] : fma2(ws2, kd[p][a], r);
           }
       }
     }
     if constexpr (INTEG == FTLE_RK4) {
       const double h6 = h / 6.0;
-      const float h6f = (float)h6;
+      const float2 h6f = bc2((float)h6);
 #pragma unroll
       for (int a = 0; a < DIM; ++a) st.c[a] = fma(h6, (double)accc[a], st.c[a]);
 #pragma unroll
-      for (int k = 0; k < K; ++k)
+      for (int p = 0; p < DIM; ++p)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a)
-          dsm[(k * DIM + a) * kBlock] =
-              fmaf(h6f, acc[(k * DIM + a) * kBlock], dsm[(k * DIM + a) * kBlock]);
+        for (int a = 0; a < DIM; ++a) {
+          const int o = (p * DIM + a) * kBlock;
+          dpl[o] = fma2(h6f, accp[o], dpl[o]);
+        }
     } else if constexpr (INTEG == FTLE_EULER) {
 #pragma unroll
       for (int a = 0; a < DIM; ++a) st.c[a] = fma(h, (double)kc[a], st.c[a]);
 #pragma unroll
-      for (int k = 0; k < K; ++k)
+      for (int p = 0; p < DIM; ++p)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a)
-          dsm[(k * DIM + a) * kBlock] = fmaf(hf, kd[k][a], dsm[(k * DIM + a) * kBlock]);
+        for (int a = 0; a < DIM; ++a) {
+          const int o = (p * DIM + a) * kBlock;
+          dpl[o] = fma2(bc2(hf), kd[p][a], dpl[o]);
+        }
     } else {  // AB2, Euler on the first step (integrate.py:240-246)
       if (i == 0) {
 #pragma unroll
         for (int a = 0; a < DIM; ++a) st.c[a] = fma(h, (double)kc[a], st.c[a]);
 #pragma unroll
-        for (int k = 0; k < K; ++k)
+        for (int p = 0; p < DIM; ++p)
 #pragma unroll
-          for (int a = 0; a < DIM; ++a)
-            dsm[(k * DIM + a) * kBlock] = fmaf(hf, kd[k][a], dsm[(k * DIM + a) * kBlock]);
+          for (int a = 0; a < DIM; ++a) {
+            const int o = (p * DIM + a) * kBlock;
+            dpl[o] = fma2(bc2(hf), kd[p][a], dpl[o]);
+          }
       } else {
 #pragma unroll
         for (int a = 0; a < DIM; ++a)
           st.c[a] = fma(h, 1.5 * (double)kc[a] - 0.5 * (double)st.kcp[a], st.c[a]);
 #pragma unroll
-        for (int k = 0; k < K; ++k)
+        for (int p = 0; p < DIM; ++p)
 #pragma unroll
-          for (int a = 0; a < DIM; ++a)
-            dsm[(k * DIM + a) * kBlock] =
-                fmaf(hf, fmaf(1.5f, kd[k][a], -0.5f * st.kdp[k][a]), dsm[(k * DIM + a) * kBlock]);
+          for (int a = 0; a < DIM; ++a) {
+            const int o = (p * DIM + a) * kBlock;
+            const float2 prev = make_float2(st.kdp[2 * p][a], st.kdp[2 * p + 1][a]);
+            dpl[o] = fma2(bc2(hf), fma2(bc2(1.5f), kd[p][a], mul2(bc2(-0.5f), prev)), dpl[o]);
+          }
       }
 #pragma unroll
       for (int a = 0; a < DIM; ++a) st.kcp[a] = kc[a];
 #pragma unroll
-      for (int k = 0; k < K; ++k)
+      for (int p = 0; p < DIM; ++p)
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) st.kdp[k][a] = kd[k][a];
+        for (int a = 0; a < DIM; ++a) {
+          st.kdp[2 * p][a] = kd[p][a].x;
+          st.kdp[2 * p + 1][a] = kd[p][a].y;
+        }
     }
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
@@ -773,9 +879,13 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
     }
   }
 #pragma unroll
-  for (int k = 0; k < K; ++k)
+  for (int p = 0; p < DIM; ++p)
 #pragma unroll
-    for (int a = 0; a < DIM; ++a) st.d[k][a] = dsm[(k * DIM + a) * kBlock];
+    for (int a = 0; a < DIM; ++a) {
+      const float2 dv = dpl[(p * DIM + a) * kBlock];
+      st.d[2 * p][a] = dv.x;
+      st.d[2 * p + 1][a] = dv.y;
+    }
 }
 
 // Final positions x_k = c + wraps*period + d_k and the FP64 FTLE epilogue.
@@ -993,8 +1103,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks<DIM>)
   extern __shared__ __align__(16) unsigned char dyn_smem[];
   const BlockSmem<DIM> sm(dyn_smem);
   float *smem_slots = sm.slots;
-  float *acc = sm.acc + threadIdx.x;
-  float *dsm = sm.d + threadIdx.x;
+  float2 *acc = reinterpret_cast<float2 *>(sm.acc) + threadIdx.x;
+  float2 *dsm = reinterpret_cast<float2 *>(sm.d) + threadIdx.x;
   const int lane = threadIdx.x & 31;
   WarpQueue<DIM> &wq = sm.queue[threadIdx.x >> 5];
   const long long N = m.w.N;
@@ -1061,8 +1171,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocksPersistent<DIM>)
   const BlockSmem<DIM> sm(dyn_smem);
   __shared__ int s_item;
   float *smem_slots = sm.slots;
-  float *acc = sm.acc + threadIdx.x;
-  float *dsm = sm.d + threadIdx.x;
+  float2 *acc = reinterpret_cast<float2 *>(sm.acc) + threadIdx.x;
+  float2 *dsm = reinterpret_cast<float2 *>(sm.d) + threadIdx.x;
   const int lane = threadIdx.x & 31;
   WarpQueue<DIM> &wq = sm.queue[threadIdx.x >> 5];
   const Header16 hd = *reinterpret_cast<const Header16 *>(m.w.snaps);
@@ -1399,14 +1509,22 @@ int ftle_windows_plan(const ftle_window *windows, int32_t count, int32_t order, 
     wins[i].reserved = 0;
   }
   // order 1: longest windows first (work items of long windows are scheduled before short
-  // ones so the tail of the persistent launch is short); order 0: as given.
+  // ones so the tail of the persistent launch is short); order 2: by the start of the
+  // window's time range (items resident together then read nearby snapshot intervals,
+  // which share L2); order 0: as given.  Insertion sorts, stable.
   int *perm = new int[count];
   for (int i = 0; i < count; ++i) perm[i] = i;
-  if (order == 1) {
-    for (int i = 1; i < count; ++i) {  // insertion sort by num_steps, descending, stable
+  auto t_first = [&](int i) {
+    const ftle_window &w = windows[i];
+    const double t_end = w.t0 + w.num_steps * w.h;
+    return w.t0 < t_end ? w.t0 : t_end;
+  };
+  if (order == 1 || order == 2) {
+    for (int i = 1; i < count; ++i) {
       const int x = perm[i];
       int k = i - 1;
-      while (k >= 0 && windows[perm[k]].num_steps < windows[x].num_steps) {
+      while (k >= 0 && (order == 1 ? windows[perm[k]].num_steps < windows[x].num_steps
+                                   : t_first(perm[k]) > t_first(x))) {
         perm[k + 1] = perm[k];
         --k;
       }

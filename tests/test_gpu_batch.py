@@ -64,7 +64,7 @@ def _alone(series, wins):
     return res
 
 
-@pytest.mark.parametrize("schedule", [Schedule(3, 1), Schedule(1, 0), Schedule(2, 1)])
+@pytest.mark.parametrize("schedule", [Schedule(3, 1), Schedule(1, 0), Schedule(2, 1), Schedule(4, 2)])
 def test_batch_equals_windows_alone(series, schedule):
     wins = _windows(np.random.default_rng(1))
     ref = _alone(series, wins)
@@ -87,7 +87,7 @@ def test_batch_graph_replay_and_autotune(series):
             r.positions.copy_(p)
 
     best = batch.autotune(prologue=reset, use_cache=False)
-    assert isinstance(best, Schedule) and len(batch.tuning) == 8  # 1..4 CTAs/SM x 2 orders
+    assert isinstance(best, Schedule) and len(batch.tuning) == 12  # 1..4 CTAs/SM x 3 orders
     batch.capture(prologue=reset)
     for _ in range(2):
         ftles = batch.replay()
