@@ -51,7 +51,8 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--workload",
-                   choices=["abc", "batched", "gyre", "abc256", "surrogate", "surrogate3d"],
+                   choices=["abc", "batched", "gyre", "abc256", "surrogate", "surrogate3d",
+                            "surrogate_sweep", "files"],
                    default="abc",
                    help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
                         "turbulence windows in one persistent launch")
@@ -85,6 +86,9 @@ def parse_args():
     p.add_argument("--kmax", type=float, default=128.0,
                    help="surrogate: largest wavenumber of the turbulence field")
     p.add_argument("--tol", type=float, default=1e-3, help="surrogate: judge tolerance")
+    p.add_argument("--files-snapshots", type=int, default=401, help="files: snapshot files")
+    p.add_argument("--files-period", type=float, default=2.5, help="files: flow-map period")
+    p.add_argument("--files-workers", type=int, default=8, help="files: reader threads")
     return p.parse_args()
 
 
@@ -329,6 +333,10 @@ def run_ours(args):
     pos = torch.empty_like(pos0)
     ftle = torch.empty(N, dtype=torch.float64, device=dev)
     series = SnapshotSeries(grid, snaps_d, precision=args.precision, periodic_time=True)
+    if args.no_plain:  # the FP64 stack is needed again only by the plain leg
+        del snaps_d
+        torch.cuda.empty_cache()
+        snaps_d = None
     kw = dict(integrator="rk4", time_mode="blend", h=w["h"], num_steps=w["num_steps"],
               map_period=w["num_steps"] * w["h"], t0=t0, snapshot_dt=w["snap_dt"])
     chunk = args.chunk_steps if (args.chunk_steps > 0 and args.precision != "fp64") else None
@@ -606,7 +614,7 @@ def run_batched(args):
     # plain FP64, one launch per window, on every 8th window (same windows' FTLE compared)
     series64 = SnapshotSeries(grid, snaps, precision="fp64")
     sel = list(range(0, 64, 8))
-    ps64, ms64, errs, ftle_stats = 0, 0.0, [], []
+    ps64, ms64, errs, ftle_stats, floors = 0, 0.0, [], [], []
     for i in sel:
         w = wins[i]
         p = pristine[i].clone()
@@ -623,6 +631,13 @@ def run_batched(args):
         ps64 += pristine[i].shape[0] * w.num_steps
         errs.append(float(torch.linalg.vector_norm(w.ftle - f64) / torch.linalg.vector_norm(f64)))
         ftle_stats.append((float(f64.mean()), float(f64.max()), w.num_steps * h))
+        # chaos floor: the same FP64 window from seeds moved by one ulp each; how far two
+        # exact-arithmetic runs that differ only in the last bit of the inputs drift apart
+        p1 = torch.nextafter(pristine[i], torch.full_like(pristine[i], math.inf))
+        f64p = run_window(series64, p1, integrator="rk4", time_mode="blend", h=h,
+                          num_steps=w.num_steps, t0=w.t0, snapshot_dt=dt)
+        floors.append(float(torch.linalg.vector_norm(f64p - f64) / torch.linalg.vector_norm(f64)))
+        del p1, f64p
     plain = ps64 / (ms64 / 1e3)
     line = {
         "metric": METRIC + " (batched windows)", "value": value, "unit": UNIT, "n_gpus": 1,
@@ -641,6 +656,7 @@ def run_batched(args):
         "plain_fp64": {"value": plain, "windows": len(sel),
                        "speedup_chosen_vs_plain": value / plain,
                        "ftle_rel_err_l2_per_window": errs,
+                       "chaos_floor_fp64_1ulp_rel_l2_per_window": floors,
                        "ftle_mean_max_T_per_window": ftle_stats},
         "gpu_launches": args.steps * 1, "clocks": clk,
     }
@@ -732,6 +748,98 @@ def run_gyre(args):
                          "ftle_rel_err_l2_vs_fp64": err,
                          "speedup_vs_fp64": ms64 / msfx}
     print(json.dumps({"metric": METRIC + " (2D double gyre)", **out}), flush=True)
+    return 0
+
+
+def run_files(args):
+    """File-fed sliding windows (the reference's CLI run: one .mat file per snapshot).
+
+    Double gyre on a 512 x 256 grid over [0,2] x [0,1], ``--files-snapshots`` snapshot
+    files at dt = 0.05 (velocity_x/velocity_y, one coordinate file, one seed file of
+    400 x 200 centroids x 4 at delta = 1e-3), flow-map period ``--files-period`` ->
+    p = T/dt + 1 snapshots per window and n - p + 1 sliding windows, HOLD RK4 (the
+    reference's semantics) on the plain FP64 path.  Times, end to end from the files
+    to the FTLE fields in host memory, the streamed feed (pinned host ring, device
+    ring of p + 2 snapshots, reads and copies overlapped with the previous window's
+    kernel) and the all-resident feed (read every file first), against the windows'
+    kernel time.  The reference itself re-reads p files per window.
+    """
+    import shutil
+    import tempfile
+
+    import torch
+    from scipy.io import savemat
+
+    from pyftle_b200 import flows
+    from pyftle_b200.scheduler import SlidingWindowRunner
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    shape = (512, 256)
+    nx, ny = shape
+    dt = 0.05
+    n = args.files_snapshots
+    pts = flows.grid_points_2d(*shape, (0.0, 2.0), (0.0, 1.0))
+    tmp = tempfile.mkdtemp(prefix="pyftle_files_")
+    try:
+        files = []
+        for i in range(n):
+            v = flows.double_gyre_velocity(i * dt, pts.T)
+            f = os.path.join(tmp, f"vel_{i:04d}.mat")
+            savemat(f, {"velocity_x": v[:, 0].reshape(ny, nx),
+                        "velocity_y": v[:, 1].reshape(ny, nx)})
+            files.append(f)
+        cf = os.path.join(tmp, "coords.mat")
+        savemat(cf, {"coordinate_x": pts[0].reshape(ny, nx),
+                     "coordinate_y": pts[1].reshape(ny, nx)})
+        pos = flows.seeds_2d(flows.centroid_grid_2d(400, 200, (0.005, 1.995), (0.005, 0.995)),
+                             1e-3)
+        N = pos.shape[0] // 4
+        pf = os.path.join(tmp, "seeds.mat")
+        savemat(pf, {"left": pos[:N], "right": pos[N:2 * N], "top": pos[2 * N:3 * N],
+                     "bottom": pos[3 * N:]})
+        out, results = {}, {}
+        for mode in ("streamed", "resident"):
+            def make():
+                return SlidingWindowRunner(files, [cf], [pf], dt,
+                                           flow_map_period=args.files_period, grid_shape=shape,
+                                           streaming=(mode == "streamed"),
+                                           workers=args.files_workers)
+            make().run()  # warm-up (page cache, CUDA context, allocator)
+            torch.cuda.synchronize()
+            best = None
+            for _ in range(max(1, args.steps)):
+                r = make()
+                t0 = time.perf_counter()
+                fields = r.run()
+                torch.cuda.synchronize()
+                sec = time.perf_counter() - t0
+                if best is None or sec < best[0]:
+                    best = (sec, r, fields)
+            sec, r, fields = best
+            p = r.window_length
+            W = len(fields)
+            ps = 4 * N * p * W
+            out[mode] = {"seconds": sec, "particle_steps_per_s_e2e": ps / sec,
+                         "ftle_fields_per_s_e2e": W / sec}
+            if mode == "streamed":
+                out[mode].update({"kernel_ms": r.stats["kernel_ms"],
+                                  "e2e_over_kernel": sec / (r.stats["kernel_ms"] / 1e3),
+                                  "first_window_wait_s": r.stats["first_window_wait_s"],
+                                  "device_ring_snapshots": r.stats["device_ring_snapshots"],
+                                  "host_ring_buffers": r.stats["host_ring_buffers"]})
+            results[mode] = fields
+        same = all(np.array_equal(a, b) for a, b in zip(results["streamed"], results["resident"]))
+        print(json.dumps({
+            "metric": METRIC + " (file-fed sliding windows)",
+            "config": {"workload": f"double gyre 512x256, {n} .mat snapshot files dt=0.05, "
+                                   f"400x200 centroids x 4, HOLD RK4, flow-map period "
+                                   f"{args.files_period} -> {p} snapshots per window, {W} windows",
+                       "workers": args.files_workers, "file_bytes": os.path.getsize(files[0])},
+            "windows": W, "snapshots_per_window": p, **out,
+            "streamed_equals_resident": same,
+            "reference_file_reads": W * p, "our_file_reads": n}), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     return 0
 
 
@@ -939,6 +1047,86 @@ def run_surrogate(args):
     return 0
 
 
+def run_surrogate_sweep(args):
+    """Bounded sweep of the flow-map network's shape on the learned-surrogate field.
+
+    Field as ``--workload surrogate`` (2D turbulence 1024^2, 400 snapshots dt = 0.05,
+    k in [4, --kmax], u_rms --urms; windows of T = 5, RK4 h = 0.025, start times from
+    the first --sur-windows snapshots).  For each network shape (hidden width, depth,
+    Fourier feature count, spatial / time frequency spread) the engine trains a net on
+    --train-samples FP64 RK4 trajectories for --train-steps Adam steps and reports the
+    network's raw FTLE error (relative L2 against the FP64 RK4 field) on 4 windows of
+    256^2 seeds.  The judge accepts a region when its error is below the tolerance
+    (1e-3 for the benchmark), so the raw error says whether any shape can pay.
+    """
+    import torch
+
+    from pyftle_b200 import SnapshotSeries, flows
+    from pyftle_b200.interpolate import GridSpec
+    from pyftle_b200.surrogate import TrainConfig, fit_flow_map, fourier_frequencies
+    from pyftle_b200.window import run_window
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n, S, dt, h, T = 1024, 400, 0.05, 0.025, 5.0
+    L = 2 * math.pi
+    turb = flows.FourierTurbulence2D(seed=7, num_modes=256, kmin=4, kmax=args.kmax,
+                                     urms=args.urms)
+    snaps = turb.snapshots_device(n, np.arange(S) * dt)
+    ax = flows.periodic_axis(n)
+    grid = GridSpec(shape=(n, n), origin=(0.0, 0.0), spacing=(ax[1], ax[1]), periodic=True)
+    s64 = SnapshotSeries(grid, snaps, precision="fp64")
+    del snaps
+    starts = np.arange(args.sur_windows) * dt
+    m = 256
+    c = (torch.arange(m, dtype=torch.float64, device="cuda") + 0.5) * (L / m)
+    Y, X = torch.meshgrid(c, c, indexing="ij")
+    cents = torch.stack((X.reshape(-1), Y.reshape(-1)), 1).contiguous()
+    evals = [float(starts[i]) for i in np.linspace(0, len(starts) - 1, 4).astype(int)]
+    refs = []
+    for t0 in evals:
+        pos = flows.seeds_2d_device(cents, 5e-4)
+        refs.append(run_window(s64, pos, integrator="rk4", time_mode="blend", h=h,
+                               num_steps=int(round(T / h)), t0=t0, snapshot_dt=dt))
+    shapes = [  # hidden, depth, frequencies, spatial sigma, time sigma
+        (256, 4, 32, 6.0, 0.3), (512, 4, 32, 6.0, 0.3), (256, 6, 32, 6.0, 0.3),
+        (256, 4, 64, 12.0, 0.3), (256, 4, 128, 24.0, 0.3), (512, 4, 128, 24.0, 0.3),
+        (512, 6, 128, 24.0, 0.3), (512, 4, 128, 48.0, 0.3), (256, 4, 32, 6.0, 1.0)]
+    rows = []
+    for hid, dep, nf, ss, ts in shapes:
+        freq = fourier_frequencies(nf, length=L, space_sigma=ss, time_sigma=ts)
+        net, fit = fit_flow_map(s64, T=T, h=h, snapshot_dt=dt, t0_values=starts,
+                                num_samples=args.train_samples, freq=freq, hidden=hid,
+                                depth=dep, cfg=TrainConfig(steps=args.train_steps,
+                                                           batch=65536, lr=2e-3))
+        errs = []
+        pts = torch.empty(m * m, 3, dtype=torch.float64, device="cuda")
+        pts[:, :2] = cents
+        for t0, ref in zip(evals, refs):
+            pts[:, 2] = t0
+            f = net.ftle(pts, T)
+            errs.append(float(torch.linalg.vector_norm(f - ref) / torch.linalg.vector_norm(ref)))
+        # forward + backward (dX and dW) GEMM work of the training steps
+        flops = 6.0 * args.train_steps * 65536 * sum(
+            a * b for a, b in zip([2 * nf] + [hid] * dep, [hid] * dep + [64]))
+        rows.append({"hidden": hid, "depth": dep, "frequencies": nf, "space_sigma": ss,
+                     "time_sigma": ts, "final_loss": fit["final_loss"],
+                     "train_s": fit["train_s"], "train_tflops": flops / fit["train_s"] / 1e12,
+                     "raw_ftle_rel_err_l2": errs,
+                     "raw_ftle_rel_err_l2_mean": float(np.mean(errs))})
+        print(json.dumps({"sweep_row": rows[-1]}), flush=True)
+        del net
+        torch.cuda.empty_cache()
+    best = min(rows, key=lambda r: r["raw_ftle_rel_err_l2_mean"])
+    print(json.dumps({"metric": "surrogate shape sweep: raw network FTLE error vs FP64 RK4",
+                      "config": {"field": f"2D turbulence 1024^2, k in [4,{args.kmax:g}], "
+                                          f"u_rms {args.urms}, T=5",
+                                 "train_samples": args.train_samples,
+                                 "train_steps": args.train_steps,
+                                 "eval": "4 windows x 256^2 seeds"},
+                      "rows": rows, "best": best}), flush=True)
+    return 0
+
+
 def run_surrogate3d(args):
     """The 3D surrogate (input (x0, y0, z0, t0), 4 x 384 SiLU, BF16) on the ABC flow.
 
@@ -1071,6 +1259,10 @@ def main():
         return run_surrogate(args)
     if args.workload == "surrogate3d":
         return run_surrogate3d(args)
+    if args.workload == "files":
+        return run_files(args)
+    if args.workload == "surrogate_sweep":
+        return run_surrogate_sweep(args)
     return run_ours(args)
 
 

@@ -9,8 +9,9 @@ Two artefacts:
   interpolator, ``src/pyftle/grid_interp/GridInterp.cpp`` of pyFTLE,
   compiled straight from the read-only reference tree with the flags of the
   reference's CMakeLists.txt (``-O3``, C++17, pybind11, no ``-march``).
-  Only built where the reference tree is present; the built module travels
-  with the repository snapshot (``oracle/_ref/`` is git-ignored).
+  Only built where the reference tree is present (``$PYFTLE_REFERENCE_ROOT``,
+  else a checkout named ``reference`` beside this repository); the built module
+  travels with the repository snapshot (``oracle/_ref/`` is git-ignored).
 
 Usage: ``python oracle/build.py [--force]``.
 """
@@ -23,7 +24,10 @@ import sys
 import sysconfig
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("PYFTLE_REFERENCE_ROOT", "/root/reference")
+# the pyFTLE source tree: $PYFTLE_REFERENCE_ROOT, else a checkout named `reference`
+# beside this repository
+REF_ROOT = os.environ.get("PYFTLE_REFERENCE_ROOT") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 REF_CPP = os.path.join(REF_ROOT, "src", "pyftle", "grid_interp", "GridInterp.cpp")
 LIB = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")

@@ -10,9 +10,10 @@ Host-side code (not the hot path), mirroring pyFTLE's ``file_readers.py``,
   back)`` concatenated in that order into ``NeighboringParticles``
   (file_readers.py:121-182);
 * ``FileBatchSource`` -- the reference's per-step protocol plus ``window_spec()``:
-  all snapshot files of a window are read by a thread pool into pinned host
-  memory and copied to the device on a side stream while later files are still
-  being read, so the fused path receives a device-resident stack;
+  all snapshot files of a window are read by a thread pool into a fixed ring of
+  pinned host buffers (``PinnedRing``) and copied to the device on a side stream
+  while later files are still being read, so the fused path receives a
+  device-resident stack;
 * ``MatWriter`` / ``VTKWriter`` / ``create_writer`` -- ``ftle_<id>.mat`` with keys
   ``ftle, x, y(, z)`` (reshaped to the grid when ``grid_shape`` is given) and VTK
   XML ``.vts`` (structured) / ``.vtp`` (point cloud), written directly
@@ -137,37 +138,94 @@ class FileBatchSource:
                           map_period=(n - 1) * abs(dt), snapshot_dt=dt)
 
 
+class PinnedRing:
+    """A fixed set of pinned host buffers that every snapshot read reuses.
+
+    File number ``ticket`` always lands in slot ``ticket % slots``: ``acquire(ticket)``
+    waits until the slot's previous file (``ticket - slots``) has been released and
+    its host-to-device copy has completed (the CUDA event given to
+    ``release_after``).  Tickets are released in order by the consumer, so readers
+    running ahead can never take each other's slots.  Pinning happens once, here,
+    not per file.
+    """
+
+    def __init__(self, slots: int, shape, dtype=torch.float64):
+        import threading
+
+        self.bufs = [torch.empty(shape, dtype=dtype).pin_memory() for _ in range(slots)]
+        self._events: List[Optional[torch.cuda.Event]] = [None] * slots
+        self._gen = [0] * slots
+        self._cv = threading.Condition()
+        self._aborted = False
+
+    def acquire(self, ticket: int) -> int:
+        n = len(self.bufs)
+        slot, want = ticket % n, ticket // n
+        with self._cv:
+            self._cv.wait_for(lambda: self._aborted or self._gen[slot] == want)
+            if self._aborted:
+                raise RuntimeError("snapshot reading was aborted")
+        ev = self._events[slot]
+        if ev is not None:
+            ev.synchronize()
+        return slot
+
+    def release_after(self, slot: int, event: Optional[torch.cuda.Event]) -> None:
+        with self._cv:
+            self._events[slot] = event
+            self._gen[slot] += 1
+            self._cv.notify_all()
+
+    def abort(self) -> None:
+        """Wake every reader waiting for a slot with an error (the consumer stopped)."""
+        with self._cv:
+            self._aborted = True
+            self._cv.notify_all()
+
+
+def read_velocity_into(path, ring: PinnedRing, ticket: int, dim: int, nodes: int) -> int:
+    """Read velocity file number ``ticket`` into its slot of ``ring``; returns the slot."""
+    v = read_velocity(path)
+    if v.shape != (dim, nodes):
+        raise ValueError(f"{path}: velocity has shape {v.shape}, expected {(dim, nodes)}")
+    slot = ring.acquire(ticket)
+    ring.bufs[slot].numpy()[...] = v
+    return slot
+
+
 def load_snapshots(files: Sequence[str], dim: int, nodes: int, workers: int = 8,
                    device=None) -> torch.Tensor:
     """Read velocity files in parallel into a (S, dim, nodes) float64 device tensor.
 
-    Files are read by a thread pool into pinned host buffers; each is copied to
-    the device on a side stream as soon as it is read, overlapping the copies
-    with the remaining reads.
+    Files are read by a thread pool into a fixed ring of pinned host buffers
+    (``workers + 2`` of them, reused); each is copied to the device on a side stream
+    as soon as it is read, overlapping the copies with the remaining reads.
     """
     device = device or torch.device("cuda", torch.cuda.current_device())
     out = torch.empty((len(files), dim, nodes), dtype=torch.float64, device=device)
+    if not len(files):
+        return out
     copy_stream = torch.cuda.Stream(device=device)
     # `out` comes from the current stream's pool: work still queued there may own
     # its memory until it finishes, so the copies wait for that work first
     copy_stream.wait_stream(torch.cuda.current_stream(device))
-    staging: List[torch.Tensor] = []
-
-    def read(path):
-        v = read_velocity(path)
-        if v.shape != (dim, nodes):
-            raise ValueError(f"{path}: velocity has shape {v.shape}, expected {(dim, nodes)}")
-        pinned = torch.empty((dim, nodes), dtype=torch.float64).pin_memory()
-        pinned.numpy()[...] = v
-        return pinned
-
+    ring = PinnedRing(min(len(files), max(1, workers) + 2), (dim, nodes))
     with ThreadPoolExecutor(max_workers=max(1, workers)) as pool:
-        futures = [pool.submit(read, f) for f in files]
-        with torch.cuda.stream(copy_stream):
-            for i, fut in enumerate(futures):
-                buf = fut.result()
-                out[i].copy_(buf, non_blocking=True)
-                staging.append(buf)  # keep pinned buffers alive until the copies finish
+        futures = [pool.submit(read_velocity_into, f, ring, i, dim, nodes)
+                   for i, f in enumerate(files)]
+        try:
+            with torch.cuda.stream(copy_stream):
+                for i, fut in enumerate(futures):
+                    slot = fut.result()
+                    out[i].copy_(ring.bufs[slot], non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(copy_stream)
+                    ring.release_after(slot, ev)
+        except BaseException:
+            ring.abort()
+            for fut in futures:
+                fut.cancel()
+            raise
     torch.cuda.current_stream(device).wait_stream(copy_stream)
     copy_stream.synchronize()
     return out

@@ -6,10 +6,13 @@ length is p = int(T/|dt|) + 1 and there are n - p + 1 overlapping windows
 (``__main__.py:111-166``); negative dt reverses the file lists
 (``__main__.py:91-109``); window i uses particle file i (cycled) and is named
 after its first snapshot file.  The reference runs each window in its own
-process and re-reads its p snapshot files; here all n snapshots are read once
-(in parallel, copied to the device while reading), packed once, and every
-window runs from that resident series -- one launch per window on the FP64
-path, or all windows in one persistent launch on the mixed path.
+process and re-reads its p snapshot files; here each snapshot is read once.
+On the FP64 path (the default, streaming) the files are read by a thread pool
+into a fixed ring of pinned buffers and copied and packed into a device ring of
+p + 2 snapshots while the previous window's kernel runs, one launch per window
+as soon as its snapshots are in place.  On the mixed path all n snapshots are
+read (in parallel, copied to the device while reading), packed once (FX15 needs
+the whole series' value range), and every window runs in one persistent launch.
 """
 
 from __future__ import annotations
@@ -32,7 +35,8 @@ class SlidingWindowRunner:
     def __init__(self, snapshot_files: List[str], coordinate_files: List[str],
                  particle_files: List[str], snapshot_timestep: float, flow_map_period: float,
                  grid_shape: tuple, integrator_name: str = "rk4", writer=None,
-                 precision: str = "fp64", periodic_space: bool = False, workers: int = 8):
+                 precision: str = "fp64", periodic_space: bool = False, workers: int = 8,
+                 streaming: bool = True, device_depth: int = 2):
         self.snapshot_files = list(snapshot_files)
         self.coordinate_files = list(coordinate_files)
         self.particle_files = list(particle_files)
@@ -44,6 +48,9 @@ class SlidingWindowRunner:
         self.precision = precision
         self.periodic_space = periodic_space
         self.workers = workers
+        self.streaming = bool(streaming)
+        self.device_depth = max(1, int(device_depth))
+        self.stats: dict = {}
         if self.timestep < 0:  # backward time: reverse the file order
             self.snapshot_files.reverse()
             self.coordinate_files.reverse()
@@ -70,6 +77,8 @@ class SlidingWindowRunner:
             return self._run_moving_grid(wins)
         points = io.read_coordinate(self.coordinate_files[0])
         grid = GridSpec.from_points(points, self.grid_shape, self.periodic_space)
+        if self.precision == "fp64" and self.streaming:
+            return self._run_streaming(wins, grid)
         snaps = io.load_snapshots(self.snapshot_files, grid.dim, grid.nodes, workers=self.workers)
         series = SnapshotSeries(grid, snaps, precision=self.precision)
         del snaps
@@ -94,6 +103,134 @@ class SlidingWindowRunner:
                                  snapshot_dt=dt).run()
         torch.cuda.synchronize()
         return self._emit(wins, particles, fields)
+
+    def _run_streaming(self, wins, grid):
+        """FP64 windows fed while they run (fixed grid, the reference's HOLD windows).
+
+        Snapshot files are read by a thread pool into a fixed ring of pinned host
+        buffers (``io.PinnedRing``), copied to the device on a side stream and packed
+        into a device ring of ``p + device_depth`` snapshot blocks, which the kernel
+        addresses modulo the ring length (``periodic_time`` with ``first_snapshot`` =
+        window index mod ring length; HOLD reads one snapshot per step).  Window i is
+        launched as soon as its p snapshots are packed; the read, copy and packing of
+        snapshot i + p (needed by window i + 1) then run while window i's kernel runs,
+        a ring block is overwritten only after the last window reading it finished,
+        and window i - 1's FTLE is copied back and emitted on the host meanwhile.
+        Device memory holds p + device_depth snapshots instead of all n.
+        """
+        import time
+        from concurrent.futures import ThreadPoolExecutor
+
+        from pyftle_b200 import _lib
+        from pyftle_b200._device import stream_ptr
+        from pyftle_b200.window import window_descriptor
+
+        t_start = time.perf_counter()
+        dim, nodes = grid.dim, grid.nodes
+        n = len(self.snapshot_files)
+        p = self.window_length
+        W = len(wins)
+        dt = self.timestep
+        dev = torch.device("cuda", torch.cuda.current_device())
+        block = int(_lib.load().ftle_packed_snapshot_bytes(dim, nodes, 1, _lib.F64))
+        R = min(n, p + self.device_depth)
+        ring_dev = torch.empty(R * block, dtype=torch.uint8, device=dev)
+        raw = [torch.empty((dim, nodes), dtype=torch.float64, device=dev) for _ in range(2)]
+        series = _RingSeries(grid, ring_dev, R)
+        comp = torch.cuda.current_stream(dev)
+        copy = torch.cuda.Stream(device=dev)
+        copy.wait_stream(comp)
+        host = io.PinnedRing(min(n, self.workers + 2), (dim, nodes))
+        packed: List[Optional[torch.cuda.Event]] = [None] * n
+        done: List[Optional[torch.cuda.Event]] = [None] * W
+        seeds = {}
+        for _, pf, _, _ in wins:
+            if pf not in seeds:
+                seeds[pf] = io.read_seed_particles_coordinates(pf)
+        N = {pf: len(part) for pf, part in seeds.items()}
+        out_pin = [torch.empty(max(N.values()), dtype=torch.float64).pin_memory()
+                   for _ in range(2)]
+        out_ev: List[Optional[torch.cuda.Event]] = [None, None]
+        ftle_dev = [torch.empty(max(N.values()), dtype=torch.float64, device=dev)
+                    for _ in range(2)]
+        kernel_ev = []
+        fields = []
+
+        pool = ThreadPoolExecutor(max_workers=max(1, self.workers))
+        futures = [pool.submit(io.read_velocity_into, f, host, j, dim, nodes)
+                   for j, f in enumerate(self.snapshot_files)]
+
+        def stage(j):
+            slot = futures[j].result()
+            with torch.cuda.stream(copy):
+                prev = j - R  # the snapshot that last used ring block j % R
+                if prev >= 0:
+                    copy.wait_event(done[min(prev, W - 1)])  # last window that read it
+                buf = raw[j % 2]
+                buf.copy_(host.bufs[slot], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy)
+                host.release_after(slot, ev)
+                _lib.call("ftle_pack_snapshots", dim, nodes, 1, 0, buf.data_ptr(), _lib.F64,
+                          ring_dev.data_ptr() + (j % R) * block, stream_ptr(copy))
+                e = torch.cuda.Event()
+                e.record(copy)
+                packed[j] = e
+
+        def emit(i):
+            _, pf, _, ident = wins[i]
+            out_ev[i % 2].synchronize()
+            arr = out_pin[i % 2][:N[pf]].numpy().copy()
+            if self.writer is not None:
+                self.writer.write(f"ftle_{ident}", arr,
+                                  seeds[pf].initial_centroid.cpu().numpy())
+            else:
+                fields.append(arr)
+
+        try:
+            for j in range(min(p, n)):
+                stage(j)
+            t_first = time.perf_counter()
+            for i, (_, pf, _, _) in enumerate(wins):
+                comp.wait_event(packed[i + p - 1])  # in order: every earlier block is packed too
+                pos = seeds[pf].positions.clone()
+                f = ftle_dev[i % 2][:N[pf]]
+                w = window_descriptor(series, pos, f, integrator=self.integrator,
+                                      time_mode="hold", h=dt, num_steps=p,
+                                      map_period=(p - 1) * abs(dt), first_snapshot=i % R,
+                                      snapshot_dt=dt)
+                k0 = torch.cuda.Event(enable_timing=True)
+                k1 = torch.cuda.Event(enable_timing=True)
+                k0.record(comp)
+                _lib.call("ftle_window_run_f64", w, stream_ptr(comp))
+                k1.record(comp)
+                kernel_ev.append((k0, k1))
+                d = torch.cuda.Event()
+                d.record(comp)
+                done[i] = d
+                out_pin[i % 2][:N[pf]].copy_(f, non_blocking=True)
+                e = torch.cuda.Event()
+                e.record(comp)
+                out_ev[i % 2] = e
+                if i + p < n:
+                    stage(i + p)  # overlaps window i
+                if i >= 1:
+                    emit(i - 1)   # overlaps window i
+            emit(W - 1)
+        except BaseException:
+            host.abort()
+            for fut in futures:
+                fut.cancel()
+            raise
+        finally:
+            pool.shutdown(wait=True)
+        torch.cuda.synchronize()
+        self.stats = {"seconds": time.perf_counter() - t_start,
+                      "first_window_wait_s": t_first - t_start,
+                      "kernel_ms": sum(a.elapsed_time(b) for a, b in kernel_ev),
+                      "windows": W, "device_ring_snapshots": R,
+                      "host_ring_buffers": len(host.bufs)}
+        return None if self.writer is not None else fields
 
     def _run_moving_grid(self, wins):
         """Coordinates change between snapshots: the reference loop, one window at a time."""
@@ -122,3 +259,18 @@ class SlidingWindowRunner:
             else:
                 out.append(arr)
         return None if self.writer is not None else out
+
+
+class _RingSeries:
+    """A device ring of FP64 snapshot blocks seen through the SnapshotSeries fields that
+    ``window_descriptor`` reads (time-periodic, so snapshot indices wrap at its length)."""
+
+    def __init__(self, grid: GridSpec, packed: torch.Tensor, length: int):
+        from pyftle_b200 import _lib
+
+        self.grid = grid
+        self.packed = packed
+        self.num_snapshots = int(length)
+        self.storage = _lib.F64
+        self.precision = "fp64"
+        self.periodic_time = True

@@ -1,7 +1,7 @@
 """Generate the golden vectors in tests/golden/ by running pyFTLE itself.
 
-Run in a container that holds the read-only pyFTLE tree (default
-``/root/reference``, override with ``PYFTLE_REFERENCE_ROOT``):
+Run where the pyFTLE source tree is available (``$PYFTLE_REFERENCE_ROOT``, else a
+checkout named ``reference`` beside this repository):
 
     python tests/golden/make_golden.py
 
@@ -40,7 +40,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF_ROOT = os.environ.get("PYFTLE_REFERENCE_ROOT", "/root/reference")
+# the pyFTLE source tree: $PYFTLE_REFERENCE_ROOT, else a checkout named `reference`
+# beside this repository
+REF_ROOT = os.environ.get("PYFTLE_REFERENCE_ROOT") or os.path.join(os.path.dirname(REPO),
+                                                                   "reference")
 
 STUBS = {
     "nptyping/__init__.py": """

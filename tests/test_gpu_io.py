@@ -88,3 +88,22 @@ def test_sliding_windows_backward_with_writer(golden, tmp_path):
                               snap_dt=-dt, first_snapshot=first, num_steps=4)
         np.testing.assert_allclose(m["ftle"].ravel(), ref, rtol=1e-12, atol=0)
     assert runner.windows()[0][3] == "vel_010"  # backward windows start from the last file
+
+
+@pytest.mark.parametrize("direction", [1, -1])
+def test_streaming_windows_equal_resident_series(golden, tmp_path, direction):
+    """The streamed feed (pinned host ring, device ring of p + depth packed snapshots
+    wrapping many times) gives the bits of the all-resident series, window by window,
+    forward and backward."""
+    d = golden("windows_2d.npz")
+    shape = tuple(d["shape"])
+    files, cf, pf = _write_case(tmp_path, d)
+    dt = float(d["dt"]) * direction
+    kw = dict(flow_map_period=2 * abs(dt), grid_shape=shape, workers=2)
+    streamed = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, device_depth=1, **kw)
+    resident = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **kw)
+    a, b = streamed.run(), resident.run()
+    assert streamed.stats["device_ring_snapshots"] == streamed.window_length + 1
+    assert len(a) == len(b) == len(files) - streamed.window_length + 1
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
