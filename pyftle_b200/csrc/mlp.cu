@@ -2,17 +2,17 @@
 //
 // GEMM: C[M x N] (+)= A[M x K] * B[N x K]^T, BF16 operands, FP32 accumulation in
 // tensor memory.  One CTA (4 warps) owns a 128 x NT tile (NT <= 128) of C:
-//   * operands are staged in shared memory as no-swizzle core matrices (8 x 16 B):
-//     an operand stored row-major (K contiguous) as K-major tiles, an operand stored
-//     transposed (its M/N index contiguous) as MN-major tiles with the descriptor's
-//     major bit set, so both are copied as 16-byte vectors with no transposition;
-//     every product of training (X W^T, dZ W, dZ^T X) and of the Jacobian tangents
-//     runs through this one kernel; rows past M (or N) are zero-filled;
-//   * loads are cp.async 16-byte copies in a 3-stage ring, so chunks c+1 and c+2
-//     are in flight while the tensor core works on chunk c;
-//   * one elected thread issues tcgen05.mma (kind::f16, M = 128, N = NT, K = 16
-//     per instruction) and commits each chunk to that stage's mbarrier, which
-//     frees the stage for the copies of chunk c + 3;
+//   * operands are staged in shared memory as no-swizzle core matrices (8 x 16 B) by
+//     TMA (cp.async.bulk.tensor 2D boxes, 16 bytes wide, no multicast): an operand
+//     stored row-major (K contiguous) as K-major tiles, an operand stored transposed
+//     (its M/N index contiguous) as MN-major tiles with the descriptor's major bit set,
+//     so neither needs a transposition; every product of training (X W^T, dZ W, dZ^T X)
+//     and of the Jacobian tangents runs through this one kernel; rows past M (or N) lie
+//     outside the tensor maps and arrive as zeros;
+//   * one elected thread is both the TMA producer and the tensor-core issuer: a 3-stage
+//     ring with a full barrier (TMA bytes) and an empty barrier (tcgen05.commit) per
+//     stage, so chunks c+1 and c+2 are in flight while the tensor core works on chunk c;
+//     it issues tcgen05.mma (kind::f16, M = 128, N = NT, K = 16 per instruction);
 //   * the epilogue reads the accumulator back with tcgen05.ld (warp w owns TMEM
 //     lanes 32w..32w+31 = tile rows) and applies one of the fused epilogues:
 //       EPI_F32        store (or, split-K, atomically add) FP32 C
@@ -26,7 +26,11 @@
 //
 // Element-wise kernels of the surrogate: Fourier features (+ their x/y tangents),
 // the MSE loss gradient, Adam, and the FTLE of the network's flow-map Jacobian.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
+
+#include <mutex>
 
 #include "common.cuh"
 #include "umma.cuh"
@@ -55,60 +59,54 @@ struct Epi {
   int accumulate;        // EPI_F32: atomically add into c
 };
 
-// Byte offset of element (r, k) of an R x kChunkK MN-major tile (no swizzle): the
-// core matrix of rows 8i..8i+7 and K 8j..8j+7 holds 8 K-rows of 16 B (8 consecutive
-// r each); K groups 128 B apart (leading byte offset), row groups kChunkK*16 B apart
-// (stride byte offset) -- the same descriptor strides as the K-major tiles.
-__device__ __forceinline__ uint32_t mn_off(int r, int k) {
-  return (uint32_t)((r >> 3) * (kChunkK * 16) + (k >> 3) * 128 + (k & 7) * 16 + (r & 7) * 2);
+// Operand staging by TMA (cp.async.bulk.tensor, no multicast: every tile is this GPU's
+// own memory).  Each operand has a 2D tensor map over its BF16 matrix; the boxes are
+// 16 bytes wide so the shared-memory tiles come out in the no-swizzle core-matrix
+// layouts the tensor core reads:
+//   K-major operand (element (r, k) at src[r*ld + k]): kChunkK/8 boxes of 8 k x R rows,
+//     tile layout [k/8][r][16 B]: core matrices 128 B apart along the rows (SBO) and
+//     R*16 B apart along K (LBO);
+//   MN-major operand (element (r, k) at src[k*ld + r]): R/8 boxes of 8 r x kChunkK k,
+//     tile layout [r/8][k][16 B]: core matrices 128 B apart along K (LBO) and
+//     kChunkK*16 B apart along the rows (SBO).
+// Rows past M (or N) lie outside the tensor map and arrive as zeros.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool valid) {
-  // src-size 0 zero-fills the 16 bytes without reading
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
-               "r"(valid ? 16 : 0)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Issue the copies of rows [r0, r0+R) x k [k0, k0+kChunkK) of a BF16 matrix with
-// `rows` rows into a smem tile; rows >= `rows` are zero-filled.  TRANS = false:
-// element (r, k) at src[r*ld + k] -> K-major tile; true: at src[k*ld + r] -> MN-major.
 template <bool TRANS>
-__device__ __forceinline__ void stage_async(uint32_t tile, const __nv_bfloat16 *__restrict__ src,
-                                            int ld, int rows, int r0, int R, int k0) {
+__device__ __forceinline__ void tma_operand(const CUtensorMap *map, uint32_t tile, int r0, int R,
+                                            int k0, uint32_t mbar) {
   if constexpr (!TRANS) {
-    for (int v = threadIdx.x; v < R * (kChunkK / 8); v += blockDim.x) {
-      const int r = v >> 3, c = v & 7;
-      const bool ok = r0 + r < rows;
-      const __nv_bfloat16 *p = ok ? src + (long long)(r0 + r) * ld + k0 + 8 * c : src;
-      cp_async16(tile + kmaj_off(r, 8 * c), p, ok);
-    }
+#pragma unroll
+    for (int j = 0; j < kChunkK / 8; ++j) tma_load_2d(tile + j * R * 16, map, k0 + 8 * j, r0, mbar);
   } else {
-    const int groups = R >> 3;
-    for (int v = threadIdx.x; v < kChunkK * groups; v += blockDim.x) {
-      const int k = v / groups, c = v - k * groups;
-      const bool ok = r0 + 8 * c < rows;
-      const __nv_bfloat16 *p = ok ? src + (long long)(k0 + k) * ld + r0 + 8 * c : src;
-      cp_async16(tile + mn_off(8 * c, k), p, ok);
-    }
+    for (int g = 0; g < R / 8; ++g) tma_load_2d(tile + g * kChunkK * 16, map, r0 + 8 * g, k0, mbar);
   }
+}
+
+// Descriptor of the K = 16 slice j of an operand tile with R rows (see the layouts above).
+template <bool TRANS>
+__device__ __forceinline__ uint64_t operand_desc(uint32_t tile, int R, int j) {
+  if constexpr (!TRANS) return smem_desc(tile + j * 2 * R * 16, R * 16, 128);
+  else return smem_desc(tile + j * 256, 128, kChunkK * 16);
 }
 
 template <bool A_T, bool B_T>
 __global__ void __launch_bounds__(128, 1)
-    gemm_bf16_kernel(const __nv_bfloat16 *__restrict__ A, int lda,
-                     const __nv_bfloat16 *__restrict__ B, int ldb, int M, int N, int K, int NT,
-                     int k_per_split, Epi epi, int *err) {
+    gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                     int M, int N, int K, int NT, int k_per_split, Epi epi, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long mbar[kStages];
+  __shared__ __align__(8) unsigned long long fullb[kStages];
+  __shared__ __align__(8) unsigned long long emptyb[kStages];
+  __shared__ __align__(8) unsigned long long doneb;
   __shared__ uint32_t tmem_slot;
+  __shared__ int s_ok;
   __shared__ float colsum_s[kMaxNT];
   const int tile_bytes = (kTileM + NT) * kChunkK * 2;
   const int m0 = blockIdx.x * kTileM;
@@ -121,63 +119,68 @@ __global__ void __launch_bounds__(128, 1)
   const uint32_t smem0 = smem_u32(smem);
 
   if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), ncols);
-  if (threadIdx.x < kStages) mbar_init(smem_u32(&mbar[threadIdx.x]), 1);
   for (int i = threadIdx.x; i < kMaxNT; i += blockDim.x) colsum_s[i] = 0.0f;
-  if (threadIdx.x == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(smem_u32(&fullb[s]), 1);
+      mbar_init(smem_u32(&emptyb[s]), 1);
+    }
+    mbar_init(smem_u32(&doneb), 1);
+    s_ok = 1;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
-  // A and B are K-major unless stored transposed (MN-major: bits 15 / 16)
-  const uint32_t idesc =
-      idesc_bf16(kTileM, NT) | (A_T ? (1u << 15) : 0u) | (B_T ? (1u << 16) : 0u);
-  const uint32_t sbo = kChunkK * 16;
 
-  auto load_chunk = [&](int c) {
-    const uint32_t sA = smem0 + (c % kStages) * tile_bytes;
-    const uint32_t sB = sA + kTileM * kChunkK * 2;
-    const int k0 = kbeg + c * kChunkK;
-    stage_async<A_T>(sA, A, lda, M, m0, kTileM, k0);
-    stage_async<B_T>(sB, B, ldb, N, n0, NT, k0);
-  };
-  for (int c = 0; c < kStages - 1; ++c) {
-    if (c < nchunks) load_chunk(c);
-    cp_async_commit();
-  }
-  bool ok = true;
-  for (int c = 0; c < nchunks; ++c) {
-    cp_async_wait<kStages - 2>();  // this thread's copies of chunk c landed
-    fence_proxy_async_smem();       // ... and are visible to the tensor core
-    if (!__syncthreads_and(ok)) {
-      ok = false;
-      break;
-    }
-    if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && nchunks > 0) {
+    // one thread: TMA producer and tensor-core issuer
+    const uint32_t idesc =
+        idesc_bf16(kTileM, NT) | (A_T ? (1u << 15) : 0u) | (B_T ? (1u << 16) : 0u);
+    auto load = [&](int c) {
+      const int s = c % kStages;
+      const uint32_t sA = smem0 + s * tile_bytes;
+      const uint32_t sB = sA + kTileM * kChunkK * 2;
+      const uint32_t fb = smem_u32(&fullb[s]);
+      const int k0 = kbeg + c * kChunkK;
+      mbar_expect_tx(fb, (uint32_t)tile_bytes);
+      tma_operand<A_T>(&tmA, sA, m0, kTileM, k0, fb);
+      tma_operand<B_T>(&tmB, sB, n0, NT, k0, fb);
+    };
+    int issued = 0;
+    for (; issued < kStages && issued < nchunks; ++issued) load(issued);
+    bool ok = true;
+    int c = 0;
+    for (; c < nchunks; ++c) {
+      if (!(ok = mbar_wait(smem_u32(&fullb[c % kStages]), (uint32_t)((c / kStages) & 1)))) break;
       fence_after_sync();
       const uint32_t sA = smem0 + (c % kStages) * tile_bytes;
       const uint32_t sB = sA + kTileM * kChunkK * 2;
 #pragma unroll
-      for (int j = 0; j < kChunkK / 16; ++j) {
-        umma(tmem, smem_desc(sA + j * 256, 128, sbo), smem_desc(sB + j * 256, 128, sbo), idesc,
+      for (int j = 0; j < kChunkK / 16; ++j)
+        umma(tmem, operand_desc<A_T>(sA, kTileM, j), operand_desc<B_T>(sB, NT, j), idesc,
              (c > 0 || j > 0) ? 1u : 0u);
+      umma_commit(smem_u32(&emptyb[c % kStages]));
+      // chunk c - 1 + kStages refills the stage chunk c - 1 used, once its MMAs are done
+      if (c >= 1 && issued < nchunks) {
+        if (!(ok = mbar_wait(smem_u32(&emptyb[(c - 1) % kStages]),
+                             (uint32_t)(((c - 1) / kStages) & 1))))
+          break;
+        load(issued++);
       }
-      umma_commit(smem_u32(&mbar[c % kStages]));
     }
-    // chunk c + kStages - 1 refills the stage chunk c - 1 used, once its MMAs are done
-    const int nc = c + kStages - 1;
-    if (nc < nchunks) {
-      if (c >= 1)
-        ok = mbar_wait(smem_u32(&mbar[(c - 1) % kStages]), (uint32_t)(((c - 1) / kStages) & 1));
-      if (ok) load_chunk(nc);
+    if (!ok) {
+      atomicExch(err, 1);
+      // every load already issued must land before the shared memory is released
+      for (int j = c; j < issued; ++j)
+        mbar_wait(smem_u32(&fullb[j % kStages]), (uint32_t)((j / kStages) & 1));
+      s_ok = 0;
     }
-    cp_async_commit();
+    umma_commit(smem_u32(&doneb));  // arrives once every MMA issued above has completed
   }
-  if (ok && nchunks > 0) {
-    // the last commit completes after every earlier MMA of this thread
-    const int c = nchunks - 1;
-    const bool done = mbar_wait(smem_u32(&mbar[c % kStages]), (uint32_t)((c / kStages) & 1));
-    ok = __syncthreads_and(done) != 0;
-  }
+  const bool done = nchunks == 0 || mbar_wait(smem_u32(&doneb), 0u);
+  const bool ok = __syncthreads_and(done && s_ok) != 0;
   fence_after_sync();
 
   if (ok && nchunks > 0) {
@@ -266,15 +269,9 @@ __global__ void __launch_bounds__(128, 1)
       for (int i = threadIdx.x; i < NT && n0 + i < N; i += blockDim.x)
         atomicAdd(epi.colsum + n0 + i, colsum_s[i]);
     }
-  } else if (!ok) {
-    if (threadIdx.x == 0) atomicExch(err, 1);
-    // let MMAs still in flight drain (bounded) before the accumulator is freed
-    if (nchunks > 0) {
-      const int c = nchunks - 1;
-      mbar_wait(smem_u32(&mbar[c % kStages]), (uint32_t)((c / kStages) & 1));
-    }
+  } else if (!ok && threadIdx.x == 0) {
+    atomicExch(err, 1);
   }
-  cp_async_wait<0>();  // no copy may land after the CTA's shared memory is released
   fence_before_sync();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, ncols);
@@ -496,6 +493,56 @@ using namespace ftle::mlp;
 
 namespace {
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library does
+// not link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+// 2D tensor map of a BF16 operand with `rows` rows (M or N) and K columns, read in the
+// boxes gemm_bf16_kernel issues: K-major (element (r, k) at src[r*ld + k]) boxes of 8 k x
+// R rows, MN-major (element (r, k) at src[k*ld + r]) boxes of 8 r x kChunkK k.
+int operand_map(CUtensorMap *map, const void *src, bool trans, int rows, int K, int ld, int R) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return FTLE_ERR_CUDA;
+  }
+  cuuint64_t dims[2], strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2], elem[2] = {1, 1};
+  if (!trans) {
+    dims[0] = (cuuint64_t)K;
+    dims[1] = (cuuint64_t)rows;
+    box[0] = 8;
+    box[1] = (cuuint32_t)R;
+  } else {
+    dims[0] = (cuuint64_t)rows;
+    dims[1] = (cuuint64_t)K;
+    box[0] = 8;
+    box[1] = (cuuint32_t)kChunkK;
+  }
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(src), dims,
+                         strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d) for a %s operand of %d x %d, ld %d", (int)r,
+              trans ? "MN-major" : "K-major", rows, K, ld);
+    return FTLE_ERR_CUDA;
+  }
+  return FTLE_OK;
+}
+
 int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int b_trans, int M,
                 int N, int K, int splits, const Epi &epi, int32_t *error_word, void *stream) {
   if (!A || !B || !error_word) return fail_invalid("null operand");
@@ -545,14 +592,17 @@ int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int
   const size_t smem = (size_t)kStages * (kTileM + NT) * kChunkK * 2;
   const dim3 grid((M + kTileM - 1) / kTileM, (N + NT - 1) / NT, splits);
   cudaStream_t st = as_stream(stream);
-  const __nv_bfloat16 *a = static_cast<const __nv_bfloat16 *>(A);
-  const __nv_bfloat16 *b = static_cast<const __nv_bfloat16 *>(B);
+  CUtensorMap tmA, tmB;
+  int rc = operand_map(&tmA, A, a_trans != 0, M, K, lda, kTileM);
+  if (rc) return rc;
+  rc = operand_map(&tmB, B, b_trans != 0, N, K, ldb, NT);
+  if (rc) return rc;
 #define GL(AT, BT)                                                                              \
   do {                                                                                          \
     cudaFuncSetAttribute(gemm_bf16_kernel<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                          (int)smem);                                                            \
     gemm_bf16_kernel<AT, BT>                                                                    \
-        <<<grid, 128, smem, st>>>(a, lda, b, ldb, M, N, K, NT, k_per_split, e, error_word);     \
+        <<<grid, 128, smem, st>>>(tmA, tmB, M, N, K, NT, k_per_split, e, error_word);           \
   } while (0)
   if (!a_trans && !b_trans)
     GL(false, false);
