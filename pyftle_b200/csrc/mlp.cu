@@ -180,7 +180,8 @@ __global__ void __launch_bounds__(128, 1)
     umma_commit(smem_u32(&doneb));  // arrives once every MMA issued above has completed
   }
   const bool done = nchunks == 0 || mbar_wait(smem_u32(&doneb), 0u);
-  const bool ok = __syncthreads_and(done && s_ok) != 0;
+  // s_ok is read after the barrier: the issuing thread wrote it before reaching it
+  const bool ok = (__syncthreads_and(done) != 0) && s_ok;
   fence_after_sync();
 
   if (ok && nchunks > 0) {

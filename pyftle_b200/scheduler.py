@@ -136,6 +136,7 @@ class SlidingWindowRunner:
         R = min(n, p + self.device_depth)
         ring_dev = torch.empty(R * block, dtype=torch.uint8, device=dev)
         raw = [torch.empty((dim, nodes), dtype=torch.float64, device=dev) for _ in range(2)]
+        node_order = torch.empty((dim, nodes), dtype=torch.float64, device=dev)
         series = _RingSeries(grid, ring_dev, R)
         comp = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(device=dev)
@@ -161,7 +162,7 @@ class SlidingWindowRunner:
                    for j, f in enumerate(self.snapshot_files)]
 
         def stage(j):
-            slot = futures[j].result()
+            slot, order = futures[j].result()
             with torch.cuda.stream(copy):
                 prev = j - R  # the snapshot that last used ring block j % R
                 if prev >= 0:
@@ -171,6 +172,8 @@ class SlidingWindowRunner:
                 ev = torch.cuda.Event()
                 ev.record(copy)
                 host.release_after(slot, ev)
+                if order is not None:  # column-major file components -> node order
+                    buf = io.to_node_order(buf, order, node_order)
                 _lib.call("ftle_pack_snapshots", dim, nodes, 1, 0, buf.data_ptr(), _lib.F64,
                           ring_dev.data_ptr() + (j % R) * block, stream_ptr(copy))
                 e = torch.cuda.Event()

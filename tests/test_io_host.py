@@ -76,3 +76,38 @@ def test_vtk_writer_roundtrip(tmp_path):
     d = io.read_vtk_xml(str(tmp_path / "ftle_p.vtp"))
     np.testing.assert_array_equal(d["ftle"], ftle[:5])
     np.testing.assert_array_equal(d["offsets"], np.arange(1, 6))
+
+
+def test_direct_mat_reader_matches_loadmat(tmp_path):
+    """The direct MAT v5 reader returns loadmat's doubles (C-order ravel of each stored
+    matrix) for 2D matrices, row vectors and three components, and hands every other
+    file (compressed, integer arrays, mismatched shapes) to loadmat."""
+    rng = np.random.default_rng(3)
+    cases = {
+        "m2": {"velocity_x": rng.random((7, 5)), "velocity_y": rng.random((7, 5))},
+        "vec": {"velocity_x": rng.random(11), "velocity_y": rng.random(11)},
+        "m3": {"velocity_x": rng.random((4, 6)), "velocity_y": rng.random((4, 6)),
+               "velocity_z": rng.random((4, 6)), "other": np.arange(3)},
+    }
+    for name, data in cases.items():
+        f = tmp_path / f"{name}.mat"
+        savemat(f, data)
+        raw = io._raw_components(f, "velocity")
+        assert raw is not None, name
+        ref = io._stack(loadmat(f), "velocity", f)
+        np.testing.assert_array_equal(io.read_velocity(f), ref)
+        # what the streamed feed ships: column-major bytes, reordered on the device
+        arrays, (rows, cols) = raw
+        shipped = np.stack(arrays).reshape(len(arrays), cols, rows).transpose(0, 2, 1)
+        np.testing.assert_array_equal(shipped.reshape(len(arrays), -1), ref)
+    fz = tmp_path / "zipped.mat"
+    savemat(fz, cases["m2"], do_compression=True)
+    assert io._raw_components(fz, "velocity") is None
+    np.testing.assert_array_equal(io.read_velocity(fz), io._stack(loadmat(fz), "velocity", fz))
+    fi = tmp_path / "ints.mat"
+    savemat(fi, {"velocity_x": np.arange(6).reshape(2, 3), "velocity_y": np.ones((2, 3))})
+    assert io._raw_components(fi, "velocity") is None
+    np.testing.assert_array_equal(io.read_velocity(fi), io._stack(loadmat(fi), "velocity", fi))
+    fm = tmp_path / "mixed.mat"
+    savemat(fm, {"velocity_x": rng.random((2, 3)), "velocity_y": rng.random((3, 2))})
+    assert io._raw_components(fm, "velocity") is None
