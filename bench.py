@@ -613,6 +613,17 @@ def run_batched(args):
     value = ps / (ms / 1e3)
     # plain FP64, one launch per window, on every 8th window (same windows' FTLE compared)
     series64 = SnapshotSeries(grid, snaps, precision="fp64")
+    # the same FP64 path on the 15-bit-quantised field (each component rounded to one of
+    # 32768 levels over its range, then used exactly): the FTLE error of quantisation alone
+    q = torch.empty_like(snaps)
+    for c in range(2):
+        v = snaps[:, c]
+        lo, hi = float(v.min()), float(v.max())
+        step = (hi - lo) / 32767.0 if hi > lo else 1.0
+        q[:, c] = lo + torch.round((v - lo) / step).clamp_(0, 32767) * step
+    series64q = SnapshotSeries(grid, q, precision="fp64")
+    del q
+    quant = []
     sel = list(range(0, 64, 8))
     ps64, ms64, errs, ftle_stats, floors = 0, 0.0, [], [], []
     for i in sel:
@@ -638,6 +649,11 @@ def run_batched(args):
                           num_steps=w.num_steps, t0=w.t0, snapshot_dt=dt)
         floors.append(float(torch.linalg.vector_norm(f64p - f64) / torch.linalg.vector_norm(f64)))
         del p1, f64p
+        pq = pristine[i].clone()
+        f64q = run_window(series64q, pq, integrator="rk4", time_mode="blend", h=h,
+                          num_steps=w.num_steps, t0=w.t0, snapshot_dt=dt)
+        quant.append(float(torch.linalg.vector_norm(f64q - f64) / torch.linalg.vector_norm(f64)))
+        del pq, f64q
     plain = ps64 / (ms64 / 1e3)
     line = {
         "metric": METRIC + " (batched windows)", "value": value, "unit": UNIT, "n_gpus": 1,
@@ -657,6 +673,7 @@ def run_batched(args):
                        "speedup_chosen_vs_plain": value / plain,
                        "ftle_rel_err_l2_per_window": errs,
                        "chaos_floor_fp64_1ulp_rel_l2_per_window": floors,
+                       "fp64_on_quantised_field_rel_l2_per_window": quant,
                        "ftle_mean_max_T_per_window": ftle_stats},
         "gpu_launches": args.steps * 1, "clocks": clk,
     }
