@@ -486,9 +486,10 @@ def run_ours(args):
     traffic = None
     try:
         prof = json.load(open(os.path.join(REPO, "profiles", "window_traffic.json")))
-        per_group = prof.get(args.precision + "_bytes_per_group")
-        if per_group is not None and chunk is not None:
-            traffic = int(per_group * N)
+        fixed = prof.get(args.precision + "_fixed_bytes")
+        per_group = prof.get(args.precision + "_per_group_bytes")
+        if fixed is not None and per_group is not None and chunk == 50:
+            traffic = int(fixed + per_group * N)
     except Exception:
         pass
     n_launch = -(-w["num_steps"] // chunk) if chunk else 1
@@ -505,8 +506,9 @@ def run_ours(args):
                 "dram_gbs": (traffic / (launch_ms / 1e3) / 1e9) if traffic else None,
                 "dram_frac": (traffic / (launch_ms / 1e3) / 1e9 / hbm_peak) if traffic else None,
                 "hbm_peak_gbs": hbm_peak, "hbm_peak_source": hbm_src,
-                "traffic_note": "DRAM bytes per chunk launch: ncu on a 128^3-group case, "
-                                "scaled by groups (profiles/window_traffic.json)",
+                "traffic_note": "DRAM bytes per 50-step chunk launch from the fixed + per-group "
+                                "model fitted to ncu captures at 64^3 and 128^3 groups "
+                                "(profiles/window_traffic.json)",
                 "kernel": "window_mixed_kernel" if elem == 2 else "window_f64_kernel",
                 "kernel_ms": kernel_ms, "launch_ms": launch_ms}
 

@@ -97,36 +97,125 @@ __device__ __forceinline__ uint64_t operand_desc(uint32_t tile, int R, int j) {
   else return smem_desc(tile + j * 256, 128, kChunkK * 16);
 }
 
+constexpr int kPStages = 4;    // TMA -> tensor-core stage ring
+constexpr int kEpiWarps = 4;   // epilogue warps: one per TMEM lane quarter
+constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
+constexpr uint32_t kAccCols = 2 * kMaxNT;          // two accumulators of up to 128 columns
+
+// Named barrier of the 128 epilogue threads (the producer and MMA warps never join it).
+__device__ __forceinline__ void epi_barrier() {
+  asm volatile("bar.sync 1, %0;" ::"n"(32 * kEpiWarps) : "memory");
+}
+
+// The fused epilogues on 8 consecutive columns [n, n+8) of one tile row.
+__device__ __forceinline__ void epilogue8(const Epi &epi, float *v, int row, bool row_ok, int n,
+                                          int lane, float *colsum8) {
+  if (epi.mode == EPI_F32 || epi.mode == EPI_BIAS_F32) {
+    if (epi.mode == EPI_BIAS_F32) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) v[i] += epi.bias[n + i];
+    }
+    if (row_ok) {
+      float *dst = epi.c + (long long)row * epi.ldc + n;
+      if (epi.accumulate) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) atomicAdd(dst + i, v[i]);
+      } else {
+        reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4 *>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+      }
+    }
+  } else if (epi.mode == EPI_BIAS_SILU) {
+    if (row_ok) {
+      float z[8];
+      uint32_t packed[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) z[i] = v[i] + epi.bias[n + i];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 hh = __floats2bfloat162_rn(z[2 * i] * sigmoidf_(z[2 * i]),
+                                                        z[2 * i + 1] * sigmoidf_(z[2 * i + 1]));
+        packed[i] = *reinterpret_cast<const uint32_t *>(&hh);
+      }
+      *reinterpret_cast<uint4 *>(epi.hout + (long long)row * epi.ldh + n) =
+          make_uint4(packed[0], packed[1], packed[2], packed[3]);
+      if (epi.zout) {
+        float *zd = epi.zout + (long long)row * epi.ldzout + n;
+        reinterpret_cast<float4 *>(zd)[0] = make_float4(z[0], z[1], z[2], z[3]);
+        reinterpret_cast<float4 *>(zd)[1] = make_float4(z[4], z[5], z[6], z[7]);
+      }
+    }
+  } else {  // EPI_DSILU
+    float g[8];
+    if (row_ok) {
+      const float *zs = epi.zin + (long long)row * epi.ldzin + n;
+      const float4 za = reinterpret_cast<const float4 *>(zs)[0];
+      const float4 zb = reinterpret_cast<const float4 *>(zs)[1];
+      const float z[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
+      uint32_t packed[4];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float sg = sigmoidf_(z[i]);
+        g[i] = v[i] * dsilu_from(z[i] * sg, sg);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 hh = __floats2bfloat162_rn(g[2 * i], g[2 * i + 1]);
+        packed[i] = *reinterpret_cast<const uint32_t *>(&hh);
+        // the bias gradient sums the values the next GEMM consumes
+        g[2 * i] = __low2float(hh);
+        g[2 * i + 1] = __high2float(hh);
+      }
+      *reinterpret_cast<uint4 *>(epi.hout + (long long)row * epi.ldh + n) =
+          make_uint4(packed[0], packed[1], packed[2], packed[3]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) g[i] = 0.0f;
+    }
+    if (colsum8) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        float s = g[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+        if (lane == 0) atomicAdd(&colsum8[i], s);
+      }
+    }
+  }
+}
+
 template <bool A_T, bool B_T>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kGemmThreads, 1)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                     int M, int N, int K, int NT, int k_per_split, Epi epi, int *err) {
+                     int M, int N, int K, int NT, int k_per_split, int tiles_m, int splits,
+                     int total, Epi epi, int *err) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long fullb[kStages];
-  __shared__ __align__(8) unsigned long long emptyb[kStages];
-  __shared__ __align__(8) unsigned long long doneb;
+  __shared__ __align__(8) unsigned long long fullb[kPStages];
+  __shared__ __align__(8) unsigned long long emptyb[kPStages];
+  __shared__ __align__(8) unsigned long long tfull[2];
+  __shared__ __align__(8) unsigned long long tempty[2];
+  __shared__ __align__(8) unsigned long long drainb;
   __shared__ uint32_t tmem_slot;
-  __shared__ int s_ok;
+  __shared__ volatile int s_abort;      // set by any role on a timed-out wait
+  __shared__ volatile int s_epi_abort;  // set and read by the epilogue warps only
   __shared__ float colsum_s[kMaxNT];
   const int tile_bytes = (kTileM + NT) * kChunkK * 2;
-  const int m0 = blockIdx.x * kTileM;
-  const int n0 = blockIdx.y * NT;
-  const int kbeg = blockIdx.z * k_per_split;
-  const int kend = min(K, kbeg + k_per_split);
-  const int nchunks = kend > kbeg ? (kend - kbeg) / kChunkK : 0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t ncols = NT <= 32 ? 32u : (NT <= 64 ? 64u : 128u);
   const uint32_t smem0 = smem_u32(smem);
 
-  if (warp == 0) tmem_alloc(smem_u32(&tmem_slot), ncols);
-  for (int i = threadIdx.x; i < kMaxNT; i += blockDim.x) colsum_s[i] = 0.0f;
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_slot), kAccCols);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kPStages; ++s) {
       mbar_init(smem_u32(&fullb[s]), 1);
       mbar_init(smem_u32(&emptyb[s]), 1);
     }
-    mbar_init(smem_u32(&doneb), 1);
-    s_ok = 1;
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&tfull[b]), 1);
+      mbar_init(smem_u32(&tempty[b]), kEpiWarps);
+    }
+    mbar_init(smem_u32(&drainb), 1);
+    s_abort = 0;
+    s_epi_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_before_sync();
@@ -134,148 +223,134 @@ __global__ void __launch_bounds__(128, 1)
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
 
-  if (threadIdx.x == 0 && nchunks > 0) {
-    // one thread: TMA producer and tensor-core issuer
-    const uint32_t idesc =
-        idesc_bf16(kTileM, NT) | (A_T ? (1u << 15) : 0u) | (B_T ? (1u << 16) : 0u);
-    auto load = [&](int c) {
-      const int s = c % kStages;
-      const uint32_t sA = smem0 + s * tile_bytes;
-      const uint32_t sB = sA + kTileM * kChunkK * 2;
-      const uint32_t fb = smem_u32(&fullb[s]);
-      const int k0 = kbeg + c * kChunkK;
-      mbar_expect_tx(fb, (uint32_t)tile_bytes);
-      tma_operand<A_T>(&tmA, sA, m0, kTileM, k0, fb);
-      tma_operand<B_T>(&tmB, sB, n0, NT, k0, fb);
-    };
-    int issued = 0;
-    for (; issued < kStages && issued < nchunks; ++issued) load(issued);
-    bool ok = true;
-    int c = 0;
-    for (; c < nchunks; ++c) {
-      if (!(ok = mbar_wait(smem_u32(&fullb[c % kStages]), (uint32_t)((c / kStages) & 1)))) break;
-      fence_after_sync();
-      const uint32_t sA = smem0 + (c % kStages) * tile_bytes;
-      const uint32_t sB = sA + kTileM * kChunkK * 2;
-#pragma unroll
-      for (int j = 0; j < kChunkK / 16; ++j)
-        umma(tmem, operand_desc<A_T>(sA, kTileM, j), operand_desc<B_T>(sB, NT, j), idesc,
-             (c > 0 || j > 0) ? 1u : 0u);
-      umma_commit(smem_u32(&emptyb[c % kStages]));
-      // chunk c - 1 + kStages refills the stage chunk c - 1 used, once its MMAs are done
-      if (c >= 1 && issued < nchunks) {
-        if (!(ok = mbar_wait(smem_u32(&emptyb[(c - 1) % kStages]),
-                             (uint32_t)(((c - 1) / kStages) & 1))))
-          break;
-        load(issued++);
-      }
-    }
-    if (!ok) {
-      atomicExch(err, 1);
-      // every load already issued must land before the shared memory is released
-      for (int j = c; j < issued; ++j)
-        mbar_wait(smem_u32(&fullb[j % kStages]), (uint32_t)((j / kStages) & 1));
-      s_ok = 0;
-    }
-    umma_commit(smem_u32(&doneb));  // arrives once every MMA issued above has completed
-  }
-  const bool done = nchunks == 0 || mbar_wait(smem_u32(&doneb), 0u);
-  // s_ok is read after the barrier: the issuing thread wrote it before reaching it
-  const bool ok = (__syncthreads_and(done) != 0) && s_ok;
-  fence_after_sync();
-
-  if (ok && nchunks > 0) {
-    const int row = m0 + 32 * warp + lane;
-    const bool row_ok = row < M;
-    for (int c = 0; c < NT; c += 8) {
-      float v[8];
-      tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, v);
-      const int n = n0 + c;
-      if (n >= N) continue;  // uniform across the CTA
-      if (epi.mode == EPI_F32 || epi.mode == EPI_BIAS_F32) {
-        if (epi.mode == EPI_BIAS_F32) {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) v[i] += epi.bias[n + i];
-        }
-        if (row_ok) {
-          float *dst = epi.c + (long long)row * epi.ldc + n;
-          if (epi.accumulate) {
-#pragma unroll
-            for (int i = 0; i < 8; ++i) atomicAdd(dst + i, v[i]);
-          } else {
-            reinterpret_cast<float4 *>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
-            reinterpret_cast<float4 *>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
-          }
-        }
-      } else if (epi.mode == EPI_BIAS_SILU) {
-        if (row_ok) {
-          float z[8];
-          uint32_t packed[4];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) z[i] = v[i] + epi.bias[n + i];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const __nv_bfloat162 hh = __floats2bfloat162_rn(z[2 * i] * sigmoidf_(z[2 * i]),
-                                                            z[2 * i + 1] * sigmoidf_(z[2 * i + 1]));
-            packed[i] = *reinterpret_cast<const uint32_t *>(&hh);
-          }
-          *reinterpret_cast<uint4 *>(epi.hout + (long long)row * epi.ldh + n) =
-              make_uint4(packed[0], packed[1], packed[2], packed[3]);
-          if (epi.zout) {
-            float *zd = epi.zout + (long long)row * epi.ldzout + n;
-            reinterpret_cast<float4 *>(zd)[0] = make_float4(z[0], z[1], z[2], z[3]);
-            reinterpret_cast<float4 *>(zd)[1] = make_float4(z[4], z[5], z[6], z[7]);
-          }
-        }
-      } else {  // EPI_DSILU
-        float g[8];
-        if (row_ok) {
-          const float *zs = epi.zin + (long long)row * epi.ldzin + n;
-          const float4 za = reinterpret_cast<const float4 *>(zs)[0];
-          const float4 zb = reinterpret_cast<const float4 *>(zs)[1];
-          const float z[8] = {za.x, za.y, za.z, za.w, zb.x, zb.y, zb.z, zb.w};
-          uint32_t packed[4];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const float sg = sigmoidf_(z[i]);
-            g[i] = v[i] * dsilu_from(z[i] * sg, sg);
-          }
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const __nv_bfloat162 hh = __floats2bfloat162_rn(g[2 * i], g[2 * i + 1]);
-            packed[i] = *reinterpret_cast<const uint32_t *>(&hh);
-            // the bias gradient sums the values the next GEMM consumes
-            g[2 * i] = __low2float(hh);
-            g[2 * i + 1] = __high2float(hh);
-          }
-          *reinterpret_cast<uint4 *>(epi.hout + (long long)row * epi.ldh + n) =
-              make_uint4(packed[0], packed[1], packed[2], packed[3]);
-        } else {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) g[i] = 0.0f;
-        }
-        if (epi.colsum) {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            float s = g[i];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-            if (lane == 0) atomicAdd(&colsum_s[c + i], s);
-          }
-        }
-      }
-    }
-    if (epi.mode == EPI_DSILU && epi.colsum) {
-      __syncthreads();
-      for (int i = threadIdx.x; i < NT && n0 + i < N; i += blockDim.x)
-        atomicAdd(epi.colsum + n0 + i, colsum_s[i]);
-    }
-  } else if (!ok && threadIdx.x == 0) {
+  // work unit u -> (k split, m tile, n tile); consecutive units share the n tile's B
+  auto unit = [&](int u, int &m0, int &n0, int &kbeg, int &nch) {
+    const int s = u % splits;
+    const int t = u / splits;
+    m0 = (t % tiles_m) * kTileM;
+    n0 = (t / tiles_m) * NT;
+    kbeg = s * k_per_split;
+    const int kend = min(K, kbeg + k_per_split);
+    nch = kend > kbeg ? (kend - kbeg) / kChunkK : 0;
+  };
+  auto fail = [&]() {
+    s_abort = 1;
     atomicExch(err, 1);
+  };
+
+  if (warp == 0) {
+    // ---- TMA producer: every chunk of every unit of this CTA into the stage ring
+    if (lane == 0) {
+      int g = 0;
+      for (int u = blockIdx.x; u < total && !s_abort; u += gridDim.x) {
+        int m0, n0, kbeg, nch;
+        unit(u, m0, n0, kbeg, nch);
+        for (int c = 0; c < nch; ++c, ++g) {
+          const int st = g % kPStages;
+          if (!mbar_wait(smem_u32(&emptyb[st]), (uint32_t)(((g / kPStages) & 1) ^ 1)) ||
+              s_abort) {
+            fail();
+            break;
+          }
+          const uint32_t sA = smem0 + st * tile_bytes;
+          const uint32_t sB = sA + kTileM * kChunkK * 2;
+          const uint32_t fb = smem_u32(&fullb[st]);
+          mbar_expect_tx(fb, (uint32_t)tile_bytes);
+          tma_operand<A_T>(&tmA, sA, m0, kTileM, kbeg + c * kChunkK, fb);
+          tma_operand<B_T>(&tmB, sB, n0, NT, kbeg + c * kChunkK, fb);
+        }
+      }
+      // no load may land after the shared memory is released: wait for the last ones
+      for (int j = max(0, g - kPStages); j < g; ++j)
+        mbar_wait(smem_u32(&fullb[j % kPStages]), (uint32_t)((j / kPStages) & 1));
+    }
+  } else if (warp == 1) {
+    // ---- tensor-core issuer: unit j accumulates into TMEM buffer j & 1
+    if (lane == 0) {
+      const uint32_t idesc =
+          idesc_bf16(kTileM, NT) | (A_T ? (1u << 15) : 0u) | (B_T ? (1u << 16) : 0u);
+      int g = 0, j = 0;
+      for (int u = blockIdx.x; u < total && !s_abort; u += gridDim.x, ++j) {
+        int m0, n0, kbeg, nch;
+        unit(u, m0, n0, kbeg, nch);
+        const int b = j & 1;
+        if (!mbar_wait(smem_u32(&tempty[b]), (uint32_t)(((j >> 1) & 1) ^ 1))) {
+          fail();
+          break;
+        }
+        fence_after_sync();
+        const uint32_t acc = tmem + (uint32_t)(b * kMaxNT);
+        bool ok = true;
+        for (int c = 0; c < nch; ++c, ++g) {
+          const int st = g % kPStages;
+          if (!(ok = mbar_wait(smem_u32(&fullb[st]), (uint32_t)((g / kPStages) & 1)))) break;
+          fence_after_sync();
+          const uint32_t sA = smem0 + st * tile_bytes;
+          const uint32_t sB = sA + kTileM * kChunkK * 2;
+#pragma unroll
+          for (int q = 0; q < kChunkK / 16; ++q)
+            umma(acc, operand_desc<A_T>(sA, kTileM, q), operand_desc<B_T>(sB, NT, q), idesc,
+                 (c > 0 || q > 0) ? 1u : 0u);
+          umma_commit(smem_u32(&emptyb[st]));  // the stage is free once these MMAs are done
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+        umma_commit(smem_u32(&tfull[b]));  // the accumulator is ready once they are done
+      }
+      // every MMA issued above has completed before TMEM is released
+      umma_commit(smem_u32(&drainb));
+      mbar_wait(smem_u32(&drainb), 0u);
+    }
+  } else {
+    // ---- epilogue warps: TMEM lanes 32q..32q+31 (q = warp % 4) are tile rows
+    const int q = warp & 3;
+    const int et = threadIdx.x - 64;  // 0..127 among the epilogue threads
+    int j = 0;
+    for (int u = blockIdx.x; u < total; u += gridDim.x, ++j) {
+      int m0, n0, kbeg, nch;
+      unit(u, m0, n0, kbeg, nch);
+      const int b = j & 1;
+      const bool dsum = epi.mode == EPI_DSILU && epi.colsum;
+      if (dsum) {
+        for (int i = et; i < kMaxNT; i += 32 * kEpiWarps) colsum_s[i] = 0.0f;
+        epi_barrier();
+      }
+      const bool ready = !s_epi_abort && mbar_wait(smem_u32(&tfull[b]), (uint32_t)((j >> 1) & 1));
+      if (!__all_sync(0xffffffffu, ready) && lane == 0) {
+        s_epi_abort = 1;
+        fail();
+      }
+      // the epilogue warps agree before any of them leaves (they share named barriers)
+      epi_barrier();
+      if (s_epi_abort) break;
+      fence_after_sync();
+      const int row = m0 + 32 * q + lane;
+      const bool row_ok = row < M;
+      const uint32_t tbase = tmem + (uint32_t)(b * kMaxNT) + ((uint32_t)(32 * q) << 16);
+      for (int c = 0; c < NT; c += 8) {
+        float v[8];
+        tmem_ld8(tbase + (uint32_t)c, v);
+        const int n = n0 + c;
+        if (n >= N) continue;  // uniform across the CTA
+        epilogue8(epi, v, row, row_ok, n, lane, dsum ? &colsum_s[c] : nullptr);
+      }
+      // the accumulator is drained: the issuer may reuse it
+      fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&tempty[b]));
+      if (dsum) {
+        epi_barrier();
+        for (int i = et; i < NT && n0 + i < N; i += 32 * kEpiWarps)
+          atomicAdd(epi.colsum + n0 + i, colsum_s[i]);
+        epi_barrier();
+      }
+    }
   }
   fence_before_sync();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, ncols);
+  if (warp == 1) tmem_dealloc(tmem, kAccCols);
 }
 
 // ---------------------------------------------------------------------------
@@ -590,8 +665,10 @@ int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int
   splits = (K + k_per_split - 1) / k_per_split;
   Epi e = epi;
   if (splits > 1) e.accumulate = 1;
-  const size_t smem = (size_t)kStages * (kTileM + NT) * kChunkK * 2;
-  const dim3 grid((M + kTileM - 1) / kTileM, (N + NT - 1) / NT, splits);
+  const size_t smem = (size_t)kPStages * (kTileM + NT) * kChunkK * 2;
+  const int tiles_m = (M + kTileM - 1) / kTileM, tiles_n = (N + NT - 1) / NT;
+  const int total = tiles_m * tiles_n * splits;
+  const int grid = total < kNumSMs ? total : kNumSMs;  // persistent: one CTA per SM
   cudaStream_t st = as_stream(stream);
   CUtensorMap tmA, tmB;
   int rc = operand_map(&tmA, A, a_trans != 0, M, K, lda, kTileM);
@@ -603,7 +680,8 @@ int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int
     cudaFuncSetAttribute(gemm_bf16_kernel<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                          (int)smem);                                                            \
     gemm_bf16_kernel<AT, BT>                                                                    \
-        <<<grid, 128, smem, st>>>(tmA, tmB, M, N, K, NT, k_per_split, e, error_word);           \
+        <<<grid, kGemmThreads, smem, st>>>(tmA, tmB, M, N, K, NT, k_per_split, tiles_m, splits, \
+                                           total, e, error_word);                               \
   } while (0)
   if (!a_trans && !b_trans)
     GL(false, false);
