@@ -842,8 +842,9 @@ def run_files(args):
                          "ftle_fields_per_s_e2e": W / sec}
             if mode == "streamed":
                 out[mode].update({"kernel_ms": r.stats["kernel_ms"],
+                                  "fused_kernel_ms": r.stats["fused_kernel_ms"],
                                   "e2e_over_kernel": sec / (r.stats["kernel_ms"] / 1e3),
-                                  "first_window_wait_s": r.stats["first_window_wait_s"],
+                                  "first_window_s": r.stats["first_window_s"],
                                   "device_ring_snapshots": r.stats["device_ring_snapshots"],
                                   "host_ring_buffers": r.stats["host_ring_buffers"]})
             results[mode] = fields

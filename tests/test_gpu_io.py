@@ -100,10 +100,26 @@ def test_streaming_windows_equal_resident_series(golden, tmp_path, direction):
     files, cf, pf = _write_case(tmp_path, d)
     dt = float(d["dt"]) * direction
     kw = dict(flow_map_period=2 * abs(dt), grid_shape=shape, workers=2)
-    streamed = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, device_depth=1, **kw)
     resident = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **kw)
-    a, b = streamed.run(), resident.run()
-    assert streamed.stats["device_ring_snapshots"] == streamed.window_length + 1
-    assert len(a) == len(b) == len(files) - streamed.window_length + 1
+    b = resident.run()
+    for by_steps in (True, False):  # the first window by per-step launches, or fused
+        streamed = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, device_depth=1,
+                                       first_window_per_step=by_steps, **kw)
+        a = streamed.run()
+        assert streamed.stats["device_ring_snapshots"] == streamed.window_length + 1
+        assert len(a) == len(b) == len(files) - streamed.window_length + 1
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("integrator", ["euler", "ab2"])
+def test_streaming_first_window_steps_other_integrators(golden, tmp_path, integrator):
+    d = golden("windows_2d.npz")
+    shape = tuple(d["shape"])
+    files, cf, pf = _write_case(tmp_path, d)
+    dt = float(d["dt"])
+    kw = dict(flow_map_period=3 * dt, grid_shape=shape, workers=2, integrator_name=integrator)
+    b = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **kw).run()
+    a = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, **kw).run()
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
