@@ -162,3 +162,59 @@ def test_config2_abc128_chosen_path_vs_oracle(abc128):
     rel_l2, p99 = _errors(got, f_ref)
     assert rel_l2 <= FTLE_REL_L2, rel_l2
     assert p99 <= FTLE_P99, p99
+
+
+def test_config3_turbulence_batch_vs_oracle():
+    """Config 3's field (2D random-Fourier turbulence, 256 modes, k in [4, 128], rms
+    speed 0.02, 1024^2 periodic grid, FX15 snapshots at dt = 0.05) and six uneven windows
+    in one persistent launch (RK4 h = 0.025, delta = 5e-4).  Two of them are checked
+    against the oracle on 1,000 random groups each: the plain FP64 path bit-exact, the
+    batched FX15 windows within 1e-3 (relative L2).  The oracle gets only the snapshots
+    of each window's time range (snapshot index offset by the window's first one)."""
+    from pyftle_b200.batch import WindowBatch, WindowSpecRun
+
+    n, dt, h = 1024, 0.05, 0.025
+    L = 2 * math.pi
+    turb = flows.FourierTurbulence2D(seed=7, num_modes=256, kmin=4, kmax=128, urms=0.02)
+    S = 280
+    snaps_d = turb.snapshots_device(n, np.arange(S) * dt)
+    ax = flows.periodic_axis(n)
+    grid = GridSpec(shape=(n, n), origin=(0.0, 0.0), spacing=(ax[1], ax[1]), periodic=True)
+    sfx = SnapshotSeries(grid, snaps_d, precision="fx15")
+    rng = np.random.default_rng(33)
+    specs = [(512, 3.0, 80), (96, 1.1, 40), (256, 10.0, 120), (200, 5.0, 300), (64, 0.2, 20),
+             (1024, 8.0, 60)]  # (seeds per row, t0, steps)
+    runs, seeds = [], []
+    for nx, t0, steps in specs:
+        ny = max(1, nx // 2)
+        cx = (np.arange(nx) + 0.5) * (L / nx)
+        cy = (np.arange(ny) + 0.5) * (L / ny)
+        X, Y = np.meshgrid(cx, cy)
+        pos = flows.seeds_2d(np.column_stack((X.ravel(), Y.ravel())), 5e-4)
+        seeds.append(pos)
+        runs.append(WindowSpecRun(torch.as_tensor(pos, device="cuda"), t0, h, steps))
+    ftles = WindowBatch(sfx, runs, snapshot_dt=dt).run()
+    torch.cuda.synchronize()
+    gmin, gdel = np.zeros(2), np.full(2, ax[1])
+    for w in (0, 2):
+        nx, t0, steps = specs[w]
+        pos = seeds[w]
+        N = pos.shape[0] // 4
+        idx = np.sort(rng.choice(N, 1000, replace=False))
+        sub = _subset(pos, 4, N, idx)
+        s0 = int(np.floor(t0 / dt))
+        s1 = int(np.ceil((t0 + steps * h) / dt)) + 1
+        host = turb.snapshots(n, np.arange(s0, s1) * dt)
+        kw = dict(integrator="rk4", time_mode=O.BLEND, h=h, num_steps=steps, t0=t0,
+                  snap_t0=s0 * dt, snap_dt=dt, periodic_space=True, map_period=steps * h)
+        p_ref, f_ref = O.run_window(host, (n, n), gmin, gdel, sub, **kw)
+        # the oracle's own snapshots (the device-built ones agree to ~1e-12, not bitwise)
+        s64 = SnapshotSeries(grid, torch.from_numpy(host).cuda(), precision="fp64")
+        p = torch.from_numpy(sub).cuda()
+        f = run_window(s64, p, integrator="rk4", time_mode="blend", h=h, num_steps=steps, t0=t0,
+                       snapshot_t0=s0 * dt, snapshot_dt=dt, map_period=steps * h)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(p.cpu().numpy(), p_ref)
+        np.testing.assert_allclose(f.cpu().numpy(), f_ref, rtol=FTLE_RTOL_F64, atol=0)
+        rel_l2, p99 = _errors(ftles[w].cpu().numpy()[idx], f_ref)
+        assert rel_l2 <= FTLE_REL_L2, (w, rel_l2)
