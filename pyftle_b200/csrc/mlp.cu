@@ -97,8 +97,8 @@ __device__ __forceinline__ uint64_t operand_desc(uint32_t tile, int R, int j) {
   else return smem_desc(tile + j * 256, 128, kChunkK * 16);
 }
 
-constexpr int kPStages = 4;    // TMA -> tensor-core stage ring
-constexpr int kEpiWarps = 4;   // epilogue warps: one per TMEM lane quarter
+constexpr int kPStages = 3;    // TMA -> tensor-core stage ring (2 CTAs fit an SM)
+constexpr int kEpiWarps = 8;   // epilogue warps: two per TMEM lane quarter
 constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
 constexpr uint32_t kAccCols = 2 * kMaxNT;          // two accumulators of up to 128 columns
 
@@ -185,7 +185,7 @@ __device__ __forceinline__ void epilogue8(const Epi &epi, float *v, int row, boo
 }
 
 template <bool A_T, bool B_T>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+__global__ void __launch_bounds__(kGemmThreads, 2)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                      int M, int N, int K, int NT, int k_per_split, int tiles_m, int splits,
                      int total, Epi epi, int *err) {
@@ -304,9 +304,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       mbar_wait(smem_u32(&drainb), 0u);
     }
   } else {
-    // ---- epilogue warps: TMEM lanes 32q..32q+31 (q = warp % 4) are tile rows
+    // ---- epilogue warps: TMEM lanes 32q..32q+31 (q = warp % 4) are tile rows; the two
+    // warps of a lane quarter take one half of the tile's columns each
     const int q = warp & 3;
-    const int et = threadIdx.x - 64;  // 0..127 among the epilogue threads
+    const int half = (warp - 2) >> 2;
+    const int et = threadIdx.x - 64;  // 0..255 among the epilogue threads
     int j = 0;
     for (int u = blockIdx.x; u < total; u += gridDim.x, ++j) {
       int m0, n0, kbeg, nch;
@@ -329,11 +331,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       const int row = m0 + 32 * q + lane;
       const bool row_ok = row < M;
       const uint32_t tbase = tmem + (uint32_t)(b * kMaxNT) + ((uint32_t)(32 * q) << 16);
-      for (int c = 0; c < NT; c += 8) {
+      const int cw = NT / 2;  // columns per warp (a multiple of 8)
+      for (int c = half * cw; c < (half + 1) * cw; c += 8) {
         float v[8];
         tmem_ld8(tbase + (uint32_t)c, v);
         const int n = n0 + c;
-        if (n >= N) continue;  // uniform across the CTA
+        if (n >= N) continue;  // uniform across the warp
         epilogue8(epi, v, row, row_ok, n, lane, dsum ? &colsum_s[c] : nullptr);
       }
       // the accumulator is drained: the issuer may reuse it
@@ -668,7 +671,7 @@ int gemm_launch(const void *A, int lda, int a_trans, const void *B, int ldb, int
   const size_t smem = (size_t)kPStages * (kTileM + NT) * kChunkK * 2;
   const int tiles_m = (M + kTileM - 1) / kTileM, tiles_n = (N + NT - 1) / NT;
   const int total = tiles_m * tiles_n * splits;
-  const int grid = total < kNumSMs ? total : kNumSMs;  // persistent: one CTA per SM
+  const int grid = total < 2 * kNumSMs ? total : 2 * kNumSMs;  // persistent: two CTAs per SM
   cudaStream_t st = as_stream(stream);
   CUtensorMap tmA, tmB;
   int rc = operand_map(&tmA, A, a_trans != 0, M, K, lda, kTileM);
