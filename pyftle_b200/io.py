@@ -57,20 +57,15 @@ _MI_INT8, _MI_INT32, _MI_UINT32, _MI_DOUBLE, _MI_MATRIX = 1, 5, 6, 9, 14
 _MX_DOUBLE_CLASS = 6
 
 
-def _mat_doubles(path, names, optional=()) -> Optional[dict]:
-    """Real double 2D arrays ``names`` of an uncompressed little-endian MAT v5 file,
-    parsed directly: name -> (the file's doubles in MATLAB's column-major order as a flat
-    array over the file's bytes, (rows, cols)).  loadmat returns the same doubles as a
-    (rows, cols) array.  None when the file uses anything else
-    (compression, big-endian, other classes or types, missing names): the caller then
-    reads it with loadmat.  Reading a 2 MB snapshot this way takes a fraction of
-    loadmat's time and holds the GIL only while parsing the few tags."""
-    try:
-        with open(path, "rb") as f:
-            raw = f.read()
-    except OSError:
-        return None
-    if len(raw) < 136 or raw[126:128] != b"IM":
+def _mat_parse(raw, names, optional=()) -> Optional[dict]:
+    """Locate real double 2D arrays in the bytes of an uncompressed little-endian MAT v5
+    file (``raw``: bytes or a memoryview): name -> (byte offset of the data, element
+    count, (rows, cols)); the data are the matrix's doubles in MATLAB's column-major
+    order, 8-byte aligned.  loadmat returns the same doubles as a (rows, cols) array.
+    None when the file uses anything else (compression, big-endian, other classes or
+    types, missing names): the caller then reads it with loadmat."""
+    n = len(raw)
+    if n < 136 or bytes(raw[126:128]) != b"IM":
         return None
     want = set(names)
     every = want | set(optional)
@@ -84,7 +79,7 @@ def _mat_doubles(path, names, optional=()) -> Optional[dict]:
 
     pos = 128
     try:
-        while pos + 8 <= len(raw) and every - out.keys():
+        while pos + 8 <= n and every - out.keys():
             t, nb = struct.unpack_from("<II", raw, pos)
             if t >> 16 or t != _MI_MATRIX:
                 if t >> 16 or t == 15:  # compressed elements: leave them to loadmat
@@ -103,35 +98,47 @@ def _mat_doubles(path, names, optional=()) -> Optional[dict]:
             st, snb, sd, p = sub(p)
             if st != _MI_INT8:
                 return None
-            name = raw[sd:sd + snb].decode("ascii", "replace")
+            name = bytes(raw[sd:sd + snb]).decode("ascii", "replace")
             if name in every:
                 if (flags & 0xFF) != _MX_DOUBLE_CLASS or flags & 0x800 or len(dims) != 2:
                     return None
                 st, snb, sd, p = sub(p)
                 count = dims[0] * dims[1]
-                if st != _MI_DOUBLE or snb != 8 * count or sd + snb > end:
+                if st != _MI_DOUBLE or snb != 8 * count or sd + snb > min(end, n) or sd % 8:
                     return None
-                # column-major (dims[0] x dims[1]) as stored by MATLAB / savemat
-                out[name] = (np.frombuffer(raw, dtype="<f8", count=count, offset=sd),
-                             (dims[0], dims[1]))
+                out[name] = (sd, count, (dims[0], dims[1]))
             pos = pos + 8 + ((nb + 7) // 8) * 8
     except (struct.error, ValueError):
         return None
     return out if not (want - out.keys()) else None
 
 
+def _component_layout(parsed, prefix: str):
+    """[(offset, count)] of prefix_x/y(/z) and their common (rows, cols), or None."""
+    if parsed is None:
+        return None
+    comps = [parsed[f"{prefix}_x"], parsed[f"{prefix}_y"]]
+    if f"{prefix}_z" in parsed:
+        comps.append(parsed[f"{prefix}_z"])
+    if any(c[2] != comps[0][2] for c in comps):
+        return None
+    return [(off, cnt) for off, cnt, _ in comps], comps[0][2]
+
+
 def _raw_components(file_path, prefix: str):
     """The file's ``prefix_x/y(/z)`` as column-major flat arrays with their common
     (rows, cols), or None (a file the direct reader does not take)."""
-    fast = _mat_doubles(file_path, [f"{prefix}_x", f"{prefix}_y"], [f"{prefix}_z"])
-    if fast is None:
+    try:
+        with open(file_path, "rb") as f:
+            raw = f.read()
+    except OSError:
         return None
-    comps = [fast[f"{prefix}_x"], fast[f"{prefix}_y"]]
-    if f"{prefix}_z" in fast:
-        comps.append(fast[f"{prefix}_z"])
-    if any(d != comps[0][1] for _, d in comps):
+    lay = _component_layout(_mat_parse(raw, [f"{prefix}_x", f"{prefix}_y"], [f"{prefix}_z"]),
+                            prefix)
+    if lay is None:
         return None
-    return [a for a, _ in comps], comps[0][1]
+    spans, order = lay
+    return [np.frombuffer(raw, dtype="<f8", count=cnt, offset=off) for off, cnt in spans], order
 
 
 def _read_stack(file_path, prefix: str) -> np.ndarray:
@@ -273,27 +280,60 @@ class PinnedRing:
             self._cv.notify_all()
 
 
-def read_velocity_into(path, ring: PinnedRing, ticket: int, dim: int, nodes: int):
-    """Read velocity file number ``ticket`` into its slot of ``ring``.
+def snapshot_slot_bytes(files: Sequence[str], dim: int, nodes: int) -> int:
+    """Bytes of a ring slot that holds any of ``files`` whole (or their values)."""
+    size = dim * nodes * 8
+    for f in files:
+        try:
+            size = max(size, os.path.getsize(f))
+        except OSError:
+            pass
+    return (size + 4095) // 4096 * 4096
 
-    Returns (slot, order): order None when the slot holds each component in the
-    reference's node order (the C-order ravel of the stored matrix), or (rows, cols)
-    when it holds the file's column-major bytes as they are (a plain copy, no host
-    transposition); ``to_node_order`` then reorders the device copy."""
-    raw = _raw_components(path, "velocity")
-    if raw is not None and len(raw[0]) == dim and raw[0][0].size == nodes:
-        arrays, order = raw
-        slot = ring.acquire(ticket)
-        buf = ring.bufs[slot].numpy()
-        for c in range(dim):
-            buf[c] = arrays[c]
-        return slot, order
+
+def read_velocity_into(path, ring: PinnedRing, ticket: int, dim: int, nodes: int):
+    """Read velocity file number ``ticket`` into its slot of ``ring`` (a ring of pinned
+    byte buffers).
+
+    Returns (slot, layout).  An uncompressed MAT v5 file is read whole, straight into
+    the slot (one readinto, no host-side copy); layout is then ([(byte offset,
+    count)] of each component, (rows, cols)) -- the components' column-major doubles
+    inside the slot, which ``slot_to_device`` copies and reorders on the device.  Any
+    other file goes through loadmat and the slot holds (dim, nodes) float64 values in
+    node order at offset 0 (layout None)."""
+    slot = ring.acquire(ticket)
+    buf = ring.bufs[slot]
+    try:
+        with open(path, "rb") as f:
+            got = f.readinto(memoryview(buf.numpy()))
+            whole = f.read(1) == b""
+    except OSError:
+        got, whole = 0, False
+    if whole:
+        mv = memoryview(buf.numpy())[:got]
+        lay = _component_layout(_mat_parse(mv, ["velocity_x", "velocity_y"], ["velocity_z"]),
+                                "velocity")
+        if lay is not None and len(lay[0]) == dim and all(c == nodes for _, c in lay[0]):
+            return slot, lay
     v = read_velocity(path)
     if v.shape != (dim, nodes):
         raise ValueError(f"{path}: velocity has shape {v.shape}, expected {(dim, nodes)}")
-    slot = ring.acquire(ticket)
-    ring.bufs[slot].numpy()[...] = v
+    buf[:dim * nodes * 8].view(torch.float64).numpy()[...] = v.ravel()
     return slot, None
+
+
+def slot_to_device(slot_buf: torch.Tensor, layout, dim: int, nodes: int, raw: torch.Tensor,
+                   out: torch.Tensor) -> torch.Tensor:
+    """Copy a ring slot to the device (current stream) and return it in node order
+    (``out``, (dim, nodes) float64; ``raw`` is device scratch of the same shape)."""
+    if layout is None:
+        out.copy_(slot_buf[:dim * nodes * 8].view(torch.float64).view(dim, nodes),
+                  non_blocking=True)
+        return out
+    spans, order = layout
+    for c, (off, cnt) in enumerate(spans):
+        raw[c].copy_(slot_buf[off:off + 8 * cnt].view(torch.float64), non_blocking=True)
+    return to_node_order(raw, order, out)
 
 
 def to_node_order(raw: torch.Tensor, order, out: torch.Tensor) -> torch.Tensor:
@@ -325,7 +365,8 @@ def load_snapshots(files: Sequence[str], dim: int, nodes: int, workers: int = 8,
     # `out` comes from the current stream's pool: work still queued there may own
     # its memory until it finishes, so the copies wait for that work first
     copy_stream.wait_stream(torch.cuda.current_stream(device))
-    ring = PinnedRing(min(len(files), max(1, workers) + 2), (dim, nodes))
+    ring = PinnedRing(min(len(files), max(1, workers) + 2),
+                      (snapshot_slot_bytes(files, dim, nodes),), dtype=torch.uint8)
     staging = torch.empty((dim, nodes), dtype=torch.float64, device=device)
     with ThreadPoolExecutor(max_workers=max(1, workers)) as pool:
         futures = [pool.submit(read_velocity_into, f, ring, i, dim, nodes)
@@ -333,14 +374,11 @@ def load_snapshots(files: Sequence[str], dim: int, nodes: int, workers: int = 8,
         try:
             with torch.cuda.stream(copy_stream):
                 for i, fut in enumerate(futures):
-                    slot, order = fut.result()
-                    dst = out[i] if order is None else staging
-                    dst.copy_(ring.bufs[slot], non_blocking=True)
+                    slot, layout = fut.result()
+                    slot_to_device(ring.bufs[slot], layout, dim, nodes, staging, out[i])
                     ev = torch.cuda.Event()
                     ev.record(copy_stream)
                     ring.release_after(slot, ev)
-                    if order is not None:
-                        to_node_order(staging, order, out[i])
         except BaseException:
             ring.abort()
             for fut in futures:

@@ -150,7 +150,9 @@ class SlidingWindowRunner:
         comp = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(device=dev)
         copy.wait_stream(comp)
-        host = io.PinnedRing(min(n, self.workers + 2), (dim, nodes))
+        host = io.PinnedRing(min(n, self.workers + 2),
+                             (io.snapshot_slot_bytes(self.snapshot_files, dim, nodes),),
+                             dtype=torch.uint8)
         packed: List[Optional[torch.cuda.Event]] = [None] * n
         done: List[Optional[torch.cuda.Event]] = [None] * W
         seeds = {}
@@ -171,20 +173,19 @@ class SlidingWindowRunner:
                    for j, f in enumerate(self.snapshot_files)]
 
         def stage(j):
-            slot, order = futures[j].result()
+            slot, layout = futures[j].result()
             with torch.cuda.stream(copy):
                 prev = j - R  # the snapshot that last used ring block j % R
                 if prev >= 0:
                     copy.wait_event(done[min(prev, W - 1)])  # last window that read it
-                buf = raw[j % 2]
-                buf.copy_(host.bufs[slot], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(copy)
-                host.release_after(slot, ev)
                 nb = node_bufs[j % 2]
                 if node_used[j % 2] is not None:  # a step of the first window still reads it
                     copy.wait_event(node_used[j % 2])
-                buf = io.to_node_order(buf, order, nb)  # column-major file components -> node order
+                # the file's data ranges to the device, reordered there into node order
+                buf = io.slot_to_device(host.bufs[slot], layout, dim, nodes, raw[j % 2], nb)
+                ev = torch.cuda.Event()
+                ev.record(copy)
+                host.release_after(slot, ev)
                 _lib.call("ftle_pack_snapshots", dim, nodes, 1, 0, buf.data_ptr(), _lib.F64,
                           ring_dev.data_ptr() + (j % R) * block, stream_ptr(copy))
                 e = torch.cuda.Event()
