@@ -797,19 +797,24 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
         accc[a] = s == 0 ? uc[a] : fmaf(ws, uc[a], accc[a]);
       }
       if constexpr (INTEG == FTLE_RK4) {
-        const float2 ws2 = bc2(ws);
+        // stages 1-3 keep the running sum in shared memory; the last stage's k4 goes
+        // straight into the step update below (no store and reload of the sum)
+        if (s < 3) {
+          const float2 ws2 = bc2(ws);
 #pragma unroll
-        for (int p = 0; p < DIM; ++p)
+          for (int p = 0; p < DIM; ++p)
 #pragma unroll
-          for (int a = 0; a < DIM; ++a) {
-            float2 &r = accp[(p * DIM + a) * kBlock];
-            r = s == 0 ? kd[p][a] : fma2(ws2, kd[p][a], r);
-          }
+            for (int a = 0; a < DIM; ++a) {
+              float2 &r = accp[(p * DIM + a) * kBlock];
+              r = s == 0 ? kd[p][a] : fma2(ws2, kd[p][a], r);
+            }
+        }
       }
     }
     if constexpr (INTEG == FTLE_RK4) {
       const double h6 = h / 6.0;
       const float2 h6f = bc2((float)h6);
+      const float2 one = bc2(1.0f);
 #pragma unroll
       for (int a = 0; a < DIM; ++a) st.c[a] = fma(h6, (double)accc[a], st.c[a]);
 #pragma unroll
@@ -817,7 +822,8 @@ __device__ __forceinline__ void group_advect(const MixK &m, const WinVar &v, con
 #pragma unroll
         for (int a = 0; a < DIM; ++a) {
           const int o = (p * DIM + a) * kBlock;
-          dpl[o] = fma2(h6f, accp[o], dpl[o]);
+          // k1 + 2k2 + 2k3 + k4, rounded as the in-loop fma(1, k4, sum) would
+          dpl[o] = fma2(h6f, fma2(one, kd[p][a], accp[o]), dpl[o]);
         }
     } else if constexpr (INTEG == FTLE_EULER) {
 #pragma unroll

@@ -88,7 +88,12 @@ class FTLESolver:
 
     def run(self):
         ftle = self.run_device()
-        field = ftle.cpu().numpy()
+        # back through pinned memory (torch's host allocator reuses the block; the
+        # returned array keeps it alive): ~50 GB/s instead of a pageable copy's few GB/s
+        host = torch.empty(ftle.shape, dtype=ftle.dtype, pin_memory=True)
+        host.copy_(ftle, non_blocking=True)
+        torch.cuda.current_stream(ftle.device).synchronize()
+        field = host.numpy()
         if self.output_writer is not None:
             self.output_writer.write(f"ftle_{self.source.id}", field,
                                      self.particles.initial_centroid.cpu().numpy())

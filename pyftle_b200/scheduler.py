@@ -160,11 +160,14 @@ class SlidingWindowRunner:
             if pf not in seeds:
                 seeds[pf] = io.read_seed_particles_coordinates(pf)
         N = {pf: len(part) for pf, part in seeds.items()}
+        # windows in flight: window i's FTLE is emitted while windows up to i + DEPTH - 1
+        # are queued, so host work never leaves the GPU idle between windows
+        DEPTH = 4
         out_pin = [torch.empty(max(N.values()), dtype=torch.float64).pin_memory()
-                   for _ in range(2)]
-        out_ev: List[Optional[torch.cuda.Event]] = [None, None]
+                   for _ in range(DEPTH)]
+        out_ev: List[Optional[torch.cuda.Event]] = [None] * DEPTH
         ftle_dev = [torch.empty(max(N.values()), dtype=torch.float64, device=dev)
-                    for _ in range(2)]
+                    for _ in range(DEPTH)]
         kernel_ev = []
         fields = []
 
@@ -194,8 +197,8 @@ class SlidingWindowRunner:
 
         def emit(i):
             _, pf, _, ident = wins[i]
-            out_ev[i % 2].synchronize()
-            arr = out_pin[i % 2][:N[pf]].numpy().copy()
+            out_ev[i % DEPTH].synchronize()
+            arr = out_pin[i % DEPTH][:N[pf]].numpy().copy()
             if self.writer is not None:
                 self.writer.write(f"ftle_{ident}", arr,
                                   seeds[pf].initial_centroid.cpu().numpy())
@@ -249,7 +252,7 @@ class SlidingWindowRunner:
                 _, pf, _, _ = wins[i]
                 comp.wait_event(packed[i + p - 1])  # in order: every earlier block is packed too
                 pos = seeds[pf].positions.clone()
-                f = ftle_dev[i % 2][:N[pf]]
+                f = ftle_dev[i % DEPTH][:N[pf]]
                 w = window_descriptor(series, pos, f, integrator=self.integrator,
                                       time_mode="hold", h=dt, num_steps=p,
                                       map_period=(p - 1) * abs(dt), first_snapshot=i % R,
@@ -263,15 +266,16 @@ class SlidingWindowRunner:
                 d = torch.cuda.Event()
                 d.record(comp)
                 done[i] = d
-                out_pin[i % 2][:N[pf]].copy_(f, non_blocking=True)
+                out_pin[i % DEPTH][:N[pf]].copy_(f, non_blocking=True)
                 e = torch.cuda.Event()
                 e.record(comp)
-                out_ev[i % 2] = e
+                out_ev[i % DEPTH] = e
                 if i + p < n:
-                    stage(i + p)  # overlaps window i
-                if i >= 1:
-                    emit(i - 1)   # overlaps window i
-            emit(W - 1)
+                    stage(i + p)  # overlaps the windows in flight
+                if i >= DEPTH - 1:
+                    emit(i - (DEPTH - 1))
+            for i in range(max(0, W - (DEPTH - 1)), W):
+                emit(i)
         except BaseException:
             host.abort()
             for fut in futures:
