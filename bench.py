@@ -56,7 +56,7 @@ def parse_args():
                    default="abc",
                    help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
                         "turbulence windows in one persistent launch")
-    p.add_argument("--precision", choices=["fx15", "fp16", "bf16", "fp64"], default="fx15")
+    p.add_argument("--precision", choices=["fx15", "fx16", "fp16", "bf16", "fp64"], default="fx15")
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--snapshots", type=int, default=64)
     p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
@@ -479,7 +479,7 @@ def run_ours(args):
         hbm_src = "measured"
     except Exception:
         hbm_peak, hbm_src = 6650.0, "fallback"
-    elem = 2 if args.precision in ("fx15", "fp16", "bf16") else 8
+    elem = 2 if args.precision in ("fx15", "fx16", "fp16", "bf16") else 8
     bytes_per_ps = 4 * 8 * 3 * 2 * elem  # stages x corners x comps x snapshots x elem
     achieved = bytes_per_ps * particle_steps / (kernel_ms / 1e3) / 1e9
     ceilings = gather_ceilings(dev)
@@ -883,7 +883,8 @@ def run_abc256(args):
     dt = L / S
     snaps = flows.abc_snapshots_device(ax, ax, ax, np.arange(S) * dt)
     grid = GridSpec(shape=(n, n, n), origin=(0.0,) * 3, spacing=(ax[1],) * 3, periodic=True)
-    series = SnapshotSeries(grid, snaps, precision="fx15", periodic_time=True)
+    prec = args.precision if args.precision != "fp64" else "fx15"
+    series = SnapshotSeries(grid, snaps, precision=prec, periodic_time=True)
     del snaps
     torch.cuda.empty_cache()
     # seeds: 512 x 512 x 256 centroids (meshgrid "xy" order), role-blocked, on the device
@@ -938,7 +939,8 @@ def run_abc256(args):
         "ftle_rel_err_l2_vs_fp64_max_over_windows": err,
         "ftle_rel_err_l2_vs_fp64_per_window": errs,
         "error_sample": f"every {stride}th group ({m} groups) of every window",
-        "config": {"workload": "ABC 256^3 periodic, 64 FX15 snapshots/period, 512x512x256 "
+        "precision": prec,
+        "config": {"workload": "ABC 256^3 periodic, 64 16-bit snapshots/period, 512x512x256 "
                                "centroids x 6, windows U[2,12] h=0.02, one persistent launch, "
                                "shared read-only seeds"}}), flush=True)
     return 0

@@ -17,10 +17,10 @@ LIB_PATH = os.path.join(HERE, "libpyftle_b200.so")
 FTLE_OK, FTLE_ERR_INVALID, FTLE_ERR_CUDA, FTLE_ERR_DEVICE, FTLE_ERR_UNSUPPORTED = range(5)
 EULER, AB2, RK4 = 0, 1, 2
 HOLD, BLEND = 0, 1
-F64, F16, BF16, FX15 = 0, 1, 2, 3
+F64, F16, BF16, FX15, FX16 = 0, 1, 2, 3, 4
 
 INTEGRATOR_CODES = {"euler": EULER, "ab2": AB2, "rk4": RK4}
-STORAGE_CODES = {"fp64": F64, "fp16": F16, "bf16": BF16, "fx15": FX15}
+STORAGE_CODES = {"fp64": F64, "fp16": F16, "bf16": BF16, "fx15": FX15, "fx16": FX16}
 TIME_MODES = {"hold": HOLD, "blend": BLEND}
 
 _c_dp = ctypes.c_void_p  # device pointers travel as plain addresses

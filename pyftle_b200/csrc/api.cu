@@ -124,7 +124,7 @@ int64_t ftle_packed_snapshot_bytes(int32_t dim, int64_t nodes, int32_t num_snaps
                                    int32_t storage) {
   if ((dim != 2 && dim != 3) || nodes < 0 || num_snapshots < 0) return -1;
   if (storage == FTLE_F64) return (int64_t)(2 * dim * 8) * nodes * num_snapshots;
-  if (storage == FTLE_F16 || storage == FTLE_BF16 || storage == FTLE_FX15) {
+  if (storage == FTLE_F16 || storage == FTLE_BF16 || storage == FTLE_FX15 || storage == FTLE_FX16) {
     // 256-byte decode header, then 4 or 8 16-bit values per record (3D pads each half to 4)
     const int64_t rec = dim == 2 ? 8 : 16;
     return 256 + rec * nodes * num_snapshots;
@@ -142,7 +142,7 @@ int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots, int32
   if (storage == FTLE_F64)
     return pack_snapshots_f64(dim, nodes, num_snapshots, periodic_time, src,
                               static_cast<double *>(dst), stream);
-  if (storage == FTLE_F16 || storage == FTLE_BF16 || storage == FTLE_FX15)
+  if (storage == FTLE_F16 || storage == FTLE_BF16 || storage == FTLE_FX15 || storage == FTLE_FX16)
     return pack_snapshots_16(dim, nodes, num_snapshots, periodic_time, src, storage, dst, stream);
   return fail_invalid("unknown storage %d", storage);
 }

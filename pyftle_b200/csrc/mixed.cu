@@ -157,9 +157,33 @@ __global__ void fx_finalize_kernel(Header16 *h, int dim) {
   }
 }
 
+// FX16: the FX15 decoder's byte permute turns the full 16-bit code q into
+//   f(q) = 0.5 + q/65536             for q <= 32768
+//   f(q) = 1 + (q - 32768)/32768     for q >= 32768  (bit 15 of q lands on the exponent)
+// so the range [vmin, vmax] maps onto [0.5, kFx16Top] with u = scale*f + offset.
+constexpr double kFx16Top = 2.0 - 1.0 / 32768.0;
+
+__global__ void fx16_finalize_kernel(Header16 *h, int dim) {
+  const int c = threadIdx.x;
+  if (c < dim) {
+    const double range = (double)h->vmax[c] - (double)h->vmin[c];
+    const double S = range > 0.0 ? range / (kFx16Top - 0.5) : 0.0;
+    h->scale[c] = (float)S;
+    h->offset[c] = (float)((double)h->vmin[c] - 0.5 * S);
+  }
+}
+
 template <int STORAGE>
 __device__ __forceinline__ unsigned short encode(double v, const Header16 &h, int c) {
-  if constexpr (STORAGE == FTLE_FX15) {
+  if constexpr (STORAGE == FTLE_FX16) {
+    // the code whose decoded value (with the header's FP32 scale / offset) is nearest
+    const double S = (double)h.scale[c];
+    if (!(S > 0.0)) return 0;
+    const double f = (v - (double)h.offset[c]) / S;
+    double q = f <= 1.0 ? rint((f - 0.5) * 65536.0) : 32768.0 + rint((f - 1.0) * 32768.0);
+    q = q < 0.0 ? 0.0 : (q > 65535.0 ? 65535.0 : q);
+    return (unsigned short)q;
+  } else if constexpr (STORAGE == FTLE_FX15) {
     const double range = (double)h.vmax[c] - (double)h.vmin[c];
     double q = range > 0.0 ? rint((v - (double)h.vmin[c]) * (kFxMax / range)) : 0.0;
     q = q < 0.0 ? 0.0 : (q > kFxMax ? kFxMax : q);
@@ -208,9 +232,12 @@ static int pack16(int64_t nodes, int32_t S, int32_t periodic_time, const double 
   Header16 *h = static_cast<Header16 *>(dst);
   unsigned char *recs = static_cast<unsigned char *>(dst) + kHeaderBytes;
   header_init_kernel<<<1, 32, 0, st>>>(h);
-  if constexpr (STORAGE == FTLE_FX15) {
+  if constexpr (STORAGE == FTLE_FX15 || STORAGE == FTLE_FX16) {
     minmax_kernel<DIM><<<grid_blocks(nodes * S, 256), 256, 0, st>>>(src, nodes, S, h);
-    fx_finalize_kernel<<<1, 32, 0, st>>>(h, DIM);
+    if constexpr (STORAGE == FTLE_FX15)
+      fx_finalize_kernel<<<1, 32, 0, st>>>(h, DIM);
+    else
+      fx16_finalize_kernel<<<1, 32, 0, st>>>(h, DIM);
   }
   pack16_kernel<DIM, STORAGE><<<grid_blocks(nodes * S, 256), 256, 0, st>>>(src, nodes, S,
                                                                            periodic_time, h, recs);
@@ -224,10 +251,12 @@ int pack_snapshots_16(int32_t dim, int64_t nodes, int32_t num_snapshots, int32_t
   if (dim == 2) {
     if (storage == FTLE_F16) P16(2, FTLE_F16);
     if (storage == FTLE_BF16) P16(2, FTLE_BF16);
+    if (storage == FTLE_FX16) P16(2, FTLE_FX16);
     P16(2, FTLE_FX15);
   } else {
     if (storage == FTLE_F16) P16(3, FTLE_F16);
     if (storage == FTLE_BF16) P16(3, FTLE_BF16);
+    if (storage == FTLE_FX16) P16(3, FTLE_FX16);
     P16(3, FTLE_FX15);
   }
 #undef P16
@@ -1307,8 +1336,10 @@ static void launch_any(const MixK &m, int dim, int mode, int integ, int storage,
 static int mixed_setup(const ftle_window *w, MixK &m) {
   int rc = window_to_kernel(w, &m.w);
   if (rc) return rc;
-  if (w->storage != FTLE_F16 && w->storage != FTLE_BF16 && w->storage != FTLE_FX15)
-    return fail_invalid("the mixed-precision window needs FTLE_F16, FTLE_BF16 or FTLE_FX15 storage");
+  if (w->storage != FTLE_F16 && w->storage != FTLE_BF16 && w->storage != FTLE_FX15 &&
+      w->storage != FTLE_FX16)
+    return fail_invalid(
+        "the mixed-precision window needs FTLE_F16, FTLE_BF16, FTLE_FX15 or FTLE_FX16 storage");
   if (m.w.g.nodes >= (1LL << 31))
     return fail_invalid("the mixed-precision window supports grids below 2^31 nodes");
   for (int a = 0; a < 3; ++a) {

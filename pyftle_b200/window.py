@@ -32,7 +32,7 @@ from pyftle_b200.interpolate import GridSpec
 class EngineOptions:
     """Knobs of the fused path (no reference counterpart)."""
 
-    precision: str = "fp64"      # "fp64" (plain, reference arithmetic) | "fx15" | "fp16" | "bf16"
+    precision: str = "fp64"      # "fp64" (plain, reference arithmetic) | "fx15" | "fx16" | "fp16" | "bf16"
     time_mode: str = "hold"      # "hold" (reference) | "blend"
     periodic_time: bool = False  # snapshot index wraps modulo the series length
     chunk_steps: Optional[int] = None  # mixed path: steps per launch (None: one launch)

@@ -330,7 +330,8 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-@pytest.mark.parametrize("precision,tol", [("fx15", 1e-3), ("fp16", 2e-3), ("bf16", 1.5e-2)])
+@pytest.mark.parametrize("precision,tol", [("fx15", 1e-3), ("fx16", 6e-4), ("fp16", 2e-3),
+                                           ("bf16", 1.5e-2)])
 def test_mixed_2d_double_gyre_error(precision, tol):
     shape = (256, 128)
     pts = flows.grid_points_2d(*shape)
@@ -350,7 +351,7 @@ def test_mixed_2d_double_gyre_error(precision, tol):
 
 
 @pytest.mark.parametrize("integrator", ["euler", "ab2", "rk4"])
-@pytest.mark.parametrize("precision,tol", [("fx15", 1e-3), ("fp16", 2e-3)])
+@pytest.mark.parametrize("precision,tol", [("fx15", 1e-3), ("fx16", 6e-4), ("fp16", 2e-3)])
 def test_mixed_3d_abc_error(integrator, precision, tol):
     n = 48
     ax = flows.periodic_axis(n)
@@ -479,3 +480,34 @@ def test_fx15_range_is_exact_and_repeatable_with_negative_zeros():
         lo, hi = snaps[:, c].min(), snaps[:, c].max()
         assert vmin[c] <= lo and np.nextafter(vmin[c], np.float32(np.inf)) > lo
         assert vmax[c] >= hi and np.nextafter(vmax[c], np.float32(-np.inf)) < hi
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_fx16_codes_decode_to_the_nearest_level(dim):
+    """FX16 packs each value as the 16-bit code whose decoded level (the kernels' FX15
+    byte-permute decode: 0.5 + q/65536 up to q = 32768, 1 + (q - 32768)/32768 above, then
+    scale * f + offset) is nearest, over the whole series' range."""
+    rng = np.random.default_rng(11)
+    shape = (40, 30) if dim == 2 else (12, 10, 8)
+    nodes = int(np.prod(shape))
+    S = 4
+    snaps = rng.uniform(-2.5, 3.5, (S, dim, nodes))
+    snaps[0, :, 0] = -2.5
+    snaps[1, :, 1] = 3.5
+    grid = GridSpec(shape=shape, origin=(0.0,) * dim, spacing=(1.0,) * dim)
+    series = SnapshotSeries(grid, snaps, precision="fx16")
+    raw = series.packed.cpu().numpy()
+    hdr = np.frombuffer(raw[:64].tobytes(), np.float32)
+    scale, offset = hdr[0:4].astype(np.float64), hdr[4:8].astype(np.float64)
+    rec = 8 if dim == 2 else 16
+    recs = np.frombuffer(raw[256:256 + rec * nodes * S].tobytes(), np.uint16)
+    recs = recs.reshape(S, nodes, rec // 2)
+    cols = [0, 1] if dim == 2 else [0, 1, 2]  # first half of each pair record: snapshot s
+    q = recs[:, :, cols].astype(np.float64)
+    f = np.where(q <= 32768, 0.5 + q / 65536.0, 1.0 + (q - 32768) / 32768.0)
+    for c in range(dim):
+        u = scale[c] * f[:, :, c] + offset[c]
+        v = snaps[:, c, :]
+        step = scale[c] * np.where(q[:, :, c] < 32768, 1.0 / 65536.0, 1.0 / 32768.0)
+        assert np.all(np.abs(u - v) <= 0.5 * step * (1 + 1e-6) + 1e-6 * np.abs(v)), c
+        assert (scale[c] * (2.0 - 2.0 ** -15) + offset[c]) >= v.max() - 1e-6
