@@ -163,12 +163,21 @@ class SlidingWindowRunner:
         # windows in flight: window i's FTLE is emitted while windows up to i + DEPTH - 1
         # are queued, so host work never leaves the GPU idle between windows
         DEPTH = 4
-        out_pin = [torch.empty(max(N.values()), dtype=torch.float64).pin_memory()
-                   for _ in range(DEPTH)]
+        nmax = max(N.values())
+        # fields returned in memory land straight in one pinned result array (no per-window
+        # host copy); with a writer, or a result too large to pin, a ring of DEPTH buffers
+        results = None
+        if self.writer is None and W * nmax * 8 <= (2 << 30):
+            results = torch.empty((W, nmax), dtype=torch.float64, pin_memory=True)
+        out_pin = [torch.empty(nmax, dtype=torch.float64, pin_memory=True)
+                   for _ in range(DEPTH)] if results is None else None
         out_ev: List[Optional[torch.cuda.Event]] = [None] * DEPTH
-        ftle_dev = [torch.empty(max(N.values()), dtype=torch.float64, device=dev)
-                    for _ in range(DEPTH)]
+        ftle_dev = [torch.empty(nmax, dtype=torch.float64, device=dev) for _ in range(DEPTH)]
         kernel_ev = []
+        descs = {}  # one window descriptor per particle file, re-pointed per window
+
+        def host_out(i, n):
+            return results[i, :n] if results is not None else out_pin[i % DEPTH][:n]
         fields = []
 
         pool = ThreadPoolExecutor(max_workers=max(1, self.workers))
@@ -198,7 +207,9 @@ class SlidingWindowRunner:
         def emit(i):
             _, pf, _, ident = wins[i]
             out_ev[i % DEPTH].synchronize()
-            arr = out_pin[i % DEPTH][:N[pf]].numpy().copy()
+            arr = host_out(i, N[pf]).numpy()
+            if results is None:
+                arr = arr.copy()  # the ring slot is reused
             if self.writer is not None:
                 self.writer.write(f"ftle_{ident}", arr,
                                   seeds[pf].initial_centroid.cpu().numpy())
@@ -232,7 +243,7 @@ class SlidingWindowRunner:
             d = torch.cuda.Event()
             d.record(comp)
             done[0] = d
-            out_pin[0][:N[pf]].copy_(f, non_blocking=True)
+            host_out(0, N[pf]).copy_(f, non_blocking=True)
             e = torch.cuda.Event()
             e.record(comp)
             out_ev[0] = e
@@ -253,10 +264,15 @@ class SlidingWindowRunner:
                 comp.wait_event(packed[i + p - 1])  # in order: every earlier block is packed too
                 pos = seeds[pf].positions.clone()
                 f = ftle_dev[i % DEPTH][:N[pf]]
-                w = window_descriptor(series, pos, f, integrator=self.integrator,
-                                      time_mode="hold", h=dt, num_steps=p,
-                                      map_period=(p - 1) * abs(dt), first_snapshot=i % R,
-                                      snapshot_dt=dt)
+                w = descs.get(pf)
+                if w is None:
+                    w = descs[pf] = window_descriptor(
+                        series, pos, f, integrator=self.integrator, time_mode="hold", h=dt,
+                        num_steps=p, map_period=(p - 1) * abs(dt), first_snapshot=i % R,
+                        snapshot_dt=dt)
+                w.first_snapshot = i % R
+                w.positions = pos.data_ptr()
+                w.ftle = f.data_ptr()
                 k0 = torch.cuda.Event(enable_timing=True)
                 k1 = torch.cuda.Event(enable_timing=True)
                 k0.record(comp)
@@ -266,7 +282,7 @@ class SlidingWindowRunner:
                 d = torch.cuda.Event()
                 d.record(comp)
                 done[i] = d
-                out_pin[i % DEPTH][:N[pf]].copy_(f, non_blocking=True)
+                host_out(i, N[pf]).copy_(f, non_blocking=True)
                 e = torch.cuda.Event()
                 e.record(comp)
                 out_ev[i % DEPTH] = e
