@@ -34,7 +34,7 @@ import torch
 
 from pyftle_b200 import _lib
 from pyftle_b200._device import stream_ptr
-from pyftle_b200.window import SnapshotSeries, window_descriptor
+from pyftle_b200.window import SnapshotSeries, run_window, window_descriptor
 
 TUNING_PATH = os.path.join(os.path.expanduser("~"), ".cache", "pyftle_b200", "tuning.json")
 
@@ -51,6 +51,29 @@ class WindowSpecRun:
     ftle: Optional[torch.Tensor] = None
     first_snapshot: int = 0  # HOLD windows: snapshot used by step 0
     keep_positions: bool = False  # read-only seeds (windows may share one buffer)
+
+
+@dataclass
+class JudgeReport:
+    """Per-window outcome of ``WindowBatch.run_judged``."""
+
+    errors: List[float]       # sampled relative L2 error against FP64, before any fallback
+    readvected: List[bool]    # window recomputed by the plain FP64 kernel
+    tol: float
+    sample_stride: int
+    events: tuple = ()        # CUDA events: before the batch, after it, after the judge
+
+    @property
+    def batch_ms(self) -> float:
+        """Device time of the batch launch (with its seed gather / result scatter)."""
+        self.events[2].synchronize()
+        return self.events[0].elapsed_time(self.events[1])
+
+    @property
+    def judge_ms(self) -> float:
+        """Device time of the FP64 samples and the FP64 re-advections."""
+        self.events[2].synchronize()
+        return self.events[1].elapsed_time(self.events[2])
 
 
 @dataclass(frozen=True)
@@ -140,6 +163,7 @@ class WindowBatch:
             self._win_ftle.append(torch.empty_like(w.ftle))
         self._gather()
         arr = (_lib.FtleWindow * len(self.windows))()
+        self._map_period: List[float] = []
         for i, w in enumerate(self.windows):
             pos = self._sorted[self._win_src[i]] if self.spatial_order else w.positions
             ftle = self._win_ftle[i] if self.spatial_order else w.ftle
@@ -149,6 +173,7 @@ class WindowBatch:
                 mp = (w.num_steps - 1) * abs(w.h)
             else:
                 mp = w.num_steps * abs(w.h)
+            self._map_period.append(mp)
             arr[i] = window_descriptor(series, pos, ftle, h=w.h, num_steps=w.num_steps,
                                        map_period=mp, t0=w.t0, first_snapshot=w.first_snapshot,
                                        keep_positions=w.keep_positions, **self.kw)
@@ -202,6 +227,68 @@ class WindowBatch:
             if self.spatial_order:
                 self._scatter()
         return [w.ftle for w in self.windows]
+
+    def run_judged(self, series64: SnapshotSeries, *, tol: float = 1e-3,
+                   sample_stride: int = 100, fallback: bool = True,
+                   schedule: Optional[Schedule] = None) -> "JudgeReport":
+        """Run the batch, then judge every window against plain FP64 RK4 on a sample
+        of its groups and re-advect in FP64 every window whose sampled error exceeds
+        ``tol``.
+
+        The sample of window i is every ``sample_stride``-th group starting at group
+        ``i mod sample_stride`` (1% at the default), advected by the plain FP64
+        kernel over ``series64`` (the same snapshots stored as ``"fp64"``) with the
+        window's own start, step, length and FTLE period.  The window's error is the
+        relative L2 norm ||F - F64|| / ||F64|| over the sample (the absolute norm
+        where F64 is zero there).  With ``fallback`` every window above ``tol`` is
+        recomputed by the plain FP64 kernel over all its groups, so its FTLE (and
+        its final positions, for a window that updates them) become the FP64 ones;
+        windows that advect in place keep a copy of their seeds for this, taken
+        before the run.
+        """
+        if series64.storage != _lib.F64:
+            raise ValueError("series64 must hold the snapshots as \"fp64\"")
+        if series64.grid.shape != self.series.grid.shape:
+            raise ValueError("series64 must cover the batch's grid")
+        if sample_stride < 1:
+            raise ValueError("sample_stride must be >= 1")
+        K = 2 * self.series.grid.dim
+        seeds0 = [w.positions if w.keep_positions or not fallback else w.positions.clone()
+                  for w in self.windows]
+        samples = []
+        for i, w in enumerate(self.windows):
+            n = w.positions.shape[0] // K
+            sel = torch.arange(i % sample_stride if n > i % sample_stride else 0, n,
+                               sample_stride, device=w.positions.device)
+            sub = self._view(seeds0[i])[:, sel, :]  # advanced indexing: a copy
+            samples.append((sel, sub.reshape(-1, self.series.grid.dim).contiguous()))
+        ev = tuple(torch.cuda.Event(enable_timing=True) for _ in range(3))
+        ev[0].record()
+        self.run(schedule)
+        ev[1].record()
+        kw = dict(integrator=self.kw["integrator"], time_mode=self.kw["time_mode"],
+                  snapshot_t0=self.kw["snapshot_t0"], snapshot_dt=self.kw["snapshot_dt"])
+        errors, readvected = [], []
+        for i, w in enumerate(self.windows):
+            sel, sub = samples[i]
+            win = dict(h=w.h, num_steps=w.num_steps, map_period=self._map_period[i], t0=w.t0,
+                       first_snapshot=w.first_snapshot, **kw)
+            f64 = run_window(series64, sub, **win)
+            ref = torch.linalg.vector_norm(f64)
+            diff = torch.linalg.vector_norm(w.ftle[sel] - f64)
+            err = float(diff / ref) if float(ref) > 0 else float(diff)
+            errors.append(err)
+            redo = fallback and not err <= tol  # NaN errors are re-advected too
+            if redo:
+                pos = seeds0[i]
+                run_window(series64, pos, ftle_out=w.ftle, keep_positions=w.keep_positions,
+                           **win)
+                if not w.keep_positions:
+                    w.positions.copy_(pos)
+            readvected.append(redo)
+        ev[2].record()
+        return JudgeReport(errors=errors, readvected=readvected, tol=tol,
+                           sample_stride=sample_stride, events=ev)
 
     @property
     def particle_steps(self) -> int:

@@ -271,3 +271,86 @@ def test_batch_prefix_view_of_shared_seeds_is_not_shared(series):
     assert ftles[1].numel() == n_small
     np.testing.assert_array_equal(ftles[0].cpu().numpy(), ref_big.cpu().numpy())
     np.testing.assert_array_equal(ftles[1].cpu().numpy(), ref_prefix.cpu().numpy())
+
+
+# ---------------------------------------------------------------------------
+# FP64 judge on a 1% sample of every window, FP64 re-advection of failing windows
+# ---------------------------------------------------------------------------
+
+@pytest.fixture(scope="module")
+def bf16_and_fp64():
+    turb = flows.FourierTurbulence2D(seed=3, num_modes=96, kmin=4, kmax=30)
+    snaps = turb.snapshots(N_GRID, np.arange(S) * DT)
+    ax = flows.periodic_axis(N_GRID)
+    X, Y = np.meshgrid(ax, ax)
+    grid = GridSpec.from_points(np.stack((X.ravel(), Y.ravel())), (N_GRID, N_GRID), periodic=True)
+    # BF16 storage: errors of 1e-3..1e-2, so a tolerance in between splits the windows
+    return (SnapshotSeries(grid, snaps, precision="bf16"),
+            SnapshotSeries(grid, snaps, precision="fp64"))
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_judge_readvects_exactly_the_windows_above_tolerance(bf16_and_fp64):
+    sbf, s64 = bf16_and_fp64
+    wins = _windows(np.random.default_rng(11), count=8)
+    mixed = _alone(sbf, wins)
+    fp64 = _alone(s64, wins)
+    stride = 10
+    # the judge's error of window i: groups i % stride, i % stride + stride, ...
+    expect = []
+    for i, ((_, fm), (_, f64)) in enumerate(zip(mixed, fp64)):
+        sel = np.arange(i % stride if fm.size > i % stride else 0, fm.size, stride)
+        expect.append(_rel_l2(fm[sel], f64[sel]))
+    tol = float(np.median(expect))
+    batch, runs = _batch(sbf, wins)
+    rep = batch.run_judged(s64, tol=tol, sample_stride=stride)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(rep.errors, expect, rtol=1e-12)
+    assert rep.readvected == [e > tol for e in rep.errors]
+    assert 0 < sum(rep.readvected) < len(wins)
+    for run, redo, (pm, fm), (p64, f64) in zip(runs, rep.readvected, mixed, fp64):
+        want_p, want_f = (p64, f64) if redo else (pm, fm)
+        np.testing.assert_array_equal(run.ftle.cpu().numpy(), want_f)
+        np.testing.assert_array_equal(run.positions.cpu().numpy(), want_p)
+
+
+def test_judge_without_fallback_only_reports(bf16_and_fp64):
+    sbf, s64 = bf16_and_fp64
+    wins = _windows(np.random.default_rng(12), count=4)
+    mixed = _alone(sbf, wins)
+    batch, runs = _batch(sbf, wins)
+    rep = batch.run_judged(s64, tol=0.0, fallback=False)
+    torch.cuda.synchronize()
+    assert rep.readvected == [False] * len(wins) and all(e > 0 for e in rep.errors)
+    for run, (pm, fm) in zip(runs, mixed):
+        np.testing.assert_array_equal(run.ftle.cpu().numpy(), fm)
+        np.testing.assert_array_equal(run.positions.cpu().numpy(), pm)
+
+
+def test_judge_readvects_windows_over_shared_read_only_seeds(bf16_and_fp64):
+    sbf, s64 = bf16_and_fp64
+    rng = np.random.default_rng(13)
+    seeds = torch.as_tensor(flows.seeds_2d(rng.uniform(0, 2 * math.pi, (1500, 2)), 5e-4),
+                            device="cuda")
+    seeds0 = seeds.clone()
+    specs = [(0.1, 60), (0.4, 25), (0.9, 80)]
+    runs = [WindowSpecRun(seeds, t0, 0.01, st, keep_positions=True) for t0, st in specs]
+    batch = WindowBatch(sbf, runs, snapshot_dt=DT)
+    rep = batch.run_judged(s64, tol=0.0)
+    torch.cuda.synchronize()
+    assert rep.readvected == [True] * len(specs)
+    torch.testing.assert_close(seeds, seeds0, rtol=0, atol=0)
+    for run, (t0, st) in zip(runs, specs):
+        f = run_window(s64, seeds0.clone(), integrator="rk4", time_mode="blend", h=0.01,
+                       num_steps=st, t0=t0, snapshot_dt=DT)
+        torch.testing.assert_close(run.ftle, f, rtol=0, atol=0)
+
+
+def test_judge_rejects_a_mixed_series_as_judge(bf16_and_fp64):
+    sbf, _ = bf16_and_fp64
+    batch, _ = _batch(sbf, _windows(np.random.default_rng(14), count=2))
+    with pytest.raises(ValueError, match="fp64"):
+        batch.run_judged(sbf)
