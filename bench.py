@@ -56,7 +56,7 @@ def parse_args():
                    default="abc",
                    help="abc: the 3D ABC window (default line); batched: 64 uneven 2D "
                         "turbulence windows in one persistent launch")
-    p.add_argument("--precision", choices=["fx15", "fx16", "fp16", "bf16", "fp64"], default="fx15")
+    p.add_argument("--precision", choices=["fx15", "fx16", "fp16", "bf16", "fp64"], default="fx16")
     p.add_argument("--grid", type=int, default=128)
     p.add_argument("--snapshots", type=int, default=64)
     p.add_argument("--seeds", type=int, default=256, help="centroids per axis")
@@ -556,9 +556,10 @@ def run_ours(args):
 def run_batched(args):
     """64 uneven FTLE windows over 2D random-Fourier turbulence in one persistent launch.
 
-    1024^2 periodic grid over [0, 2pi)^2, 400 FX15 snapshots at dt = 0.05; window i:
-    seed grid nx x nx/2 with nx log-uniform in [64, 1024], length U[2, 20], start
-    uniform in [0, 20 - length], RK4 h = 0.025, 4 neighbours at delta = 5e-4.
+    1024^2 periodic grid over [0, 2pi)^2, 400 16-bit (--precision) snapshots at
+    dt = 0.05; window i: seed grid nx x nx/2 with nx log-uniform in [64, 1024], length
+    U[2, 20], start uniform in [0, 20 - length], RK4 h = 0.025, 4 neighbours at
+    delta = 5e-4.
     ``--batch-snapshots`` / ``--batch-max-length`` shrink it for profiling.
     """
     import torch
@@ -577,7 +578,7 @@ def run_batched(args):
     ax = flows.periodic_axis(n)
     grid = GridSpec(shape=(n, n), origin=(0.0, 0.0), spacing=(ax[1], ax[1]), periodic=True)
     series = SnapshotSeries(grid, snaps, precision=args.precision if args.precision != "fp64"
-                            else "fx15")
+                            else "fx16")
     torch.cuda.synchronize()
     t_gen = time.time() - t_gen
     wins, pristine = [], []
@@ -618,14 +619,22 @@ def run_batched(args):
     value = ps / (ms / 1e3)
     # plain FP64, one launch per window, on every 8th window (same windows' FTLE compared)
     series64 = SnapshotSeries(grid, snaps, precision="fp64")
-    # the same FP64 path on the 15-bit-quantised field (each component rounded to one of
-    # 32768 levels over its range, then used exactly): the FTLE error of quantisation alone
+    # the same FP64 path on the quantised field (each component rounded to the storage's
+    # levels over its range -- 32768 uniform ones for FX15, FX16's 65536 two-slope ones,
+    # else FX15's -- then used exactly): the FTLE error of quantisation alone
     q = torch.empty_like(snaps)
     for c in range(2):
         v = snaps[:, c]
         lo, hi = float(v.min()), float(v.max())
-        step = (hi - lo) / 32767.0 if hi > lo else 1.0
-        q[:, c] = lo + torch.round((v - lo) / step).clamp_(0, 32767) * step
+        if series.precision == "fx16" and hi > lo:
+            top = 1.5 - 2.0 ** -15  # decoded levels span [0.5, 2 - 2^-15]
+            f = 0.5 + (v - lo) / (hi - lo) * top
+            fq = torch.where(f <= 1.0, 0.5 + torch.round((f - 0.5) * 65536.0) / 65536.0,
+                             1.0 + torch.round((f - 1.0) * 32768.0) / 32768.0)
+            q[:, c] = lo + (fq - 0.5) * ((hi - lo) / top)
+        else:
+            step = (hi - lo) / 32767.0 if hi > lo else 1.0
+            q[:, c] = lo + torch.round((v - lo) / step).clamp_(0, 32767) * step
     series64q = SnapshotSeries(grid, q, precision="fp64")
     del q
     quant = []
@@ -695,7 +704,7 @@ def run_gyre(args):
              steps) -- plain FP64, bit-exact with pyFTLE; the reference's CPU path
              timed on the same workload on the host cores.
       blend: RK4 h = 0.01 over T = 10 (1000 steps) on time-blended snapshots --
-             the chosen FX15 path vs plain FP64.
+             the chosen 16-bit path (--precision) vs plain FP64.
     """
     import torch
 
@@ -761,12 +770,13 @@ def run_gyre(args):
     blend = dict(integrator="rk4", time_mode="blend", h=0.01, num_steps=1000, snapshot_dt=dt,
                  map_period=10.0)
     ms64, f64, _ = timed(s64, blend, max(args.steps, 2))
-    sfx = SnapshotSeries(grid, d_snaps, precision="fx15")
+    prec = args.precision if args.precision != "fp64" else "fx16"
+    sfx = SnapshotSeries(grid, d_snaps, precision=prec)
     msfx, ffx, _ = timed(sfx, dict(blend, chunk_steps=100, sort_every=1), max(args.steps, 3))
     ps = 4 * N * 1000
     err = float(torch.linalg.vector_norm(ffx - f64) / torch.linalg.vector_norm(f64))
     out["blend_fp64"] = {"particle_steps_per_s": ps / (ms64 / 1e3), "ms_per_window": ms64}
-    out["blend_fx15"] = {"particle_steps_per_s": ps / (msfx / 1e3), "ms_per_window": msfx,
+    out["blend_" + prec] = {"particle_steps_per_s": ps / (msfx / 1e3), "ms_per_window": msfx,
                          "ftle_rel_err_l2_vs_fp64": err,
                          "speedup_vs_fp64": ms64 / msfx}
     print(json.dumps({"metric": METRIC + " (2D double gyre)", **out}), flush=True)
@@ -888,7 +898,7 @@ def run_abc256(args):
     dt = L / S
     snaps = flows.abc_snapshots_device(ax, ax, ax, np.arange(S) * dt)
     grid = GridSpec(shape=(n, n, n), origin=(0.0,) * 3, spacing=(ax[1],) * 3, periodic=True)
-    prec = args.precision if args.precision != "fp64" else "fx15"
+    prec = args.precision if args.precision != "fp64" else "fx16"
     series = SnapshotSeries(grid, snaps, precision=prec, periodic_time=True)
     del snaps
     torch.cuda.empty_cache()
