@@ -323,17 +323,39 @@ def read_velocity_into(path, ring: PinnedRing, ticket: int, dim: int, nodes: int
 
 
 def slot_to_device(slot_buf: torch.Tensor, layout, dim: int, nodes: int, raw: torch.Tensor,
-                   out: torch.Tensor) -> torch.Tensor:
+                   out: torch.Tensor, cache: Optional[dict] = None) -> torch.Tensor:
     """Copy a ring slot to the device (current stream) and return it in node order
-    (``out``, (dim, nodes) float64; ``raw`` is device scratch of the same shape)."""
+    (``out``, (dim, nodes) float64; ``raw`` is device scratch of the same shape).
+
+    ``cache`` (a dict the caller keeps) holds the copy plan -- the tensor views of each
+    (slot, scratch, output, layout) combination -- so a stream of files with one layout
+    builds its views once per ring slot instead of once per file."""
+    key = None
+    if cache is not None:
+        lk = None if layout is None else (tuple(layout[0]), layout[1])
+        key = (slot_buf.data_ptr(), raw.data_ptr(), out.data_ptr(), lk)
+        plan = cache.get(key)
+        if plan is not None:
+            for dst, src in plan:
+                dst.copy_(src, non_blocking=True)
+            return out
     if layout is None:
-        out.copy_(slot_buf[:dim * nodes * 8].view(torch.float64).view(dim, nodes),
-                  non_blocking=True)
-        return out
-    spans, order = layout
-    for c, (off, cnt) in enumerate(spans):
-        raw[c].copy_(slot_buf[off:off + 8 * cnt].view(torch.float64), non_blocking=True)
-    return to_node_order(raw, order, out)
+        plan = [(out, slot_buf[:dim * nodes * 8].view(torch.float64).view(dim, nodes))]
+    else:
+        spans, order = layout
+        plan = [(raw[c], slot_buf[off:off + 8 * cnt].view(torch.float64))
+                for c, (off, cnt) in enumerate(spans)]
+        if order is None:
+            if out.data_ptr() != raw.data_ptr():
+                plan.append((out, raw))
+        else:
+            rows, cols = order
+            plan.append((out.view(dim, rows, cols), raw.view(dim, cols, rows).transpose(1, 2)))
+    for dst, src in plan:
+        dst.copy_(src, non_blocking=True)
+    if key is not None:
+        cache[key] = plan
+    return out
 
 
 def to_node_order(raw: torch.Tensor, order, out: torch.Tensor) -> torch.Tensor:

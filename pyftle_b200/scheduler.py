@@ -173,8 +173,14 @@ class SlidingWindowRunner:
                    for _ in range(DEPTH)] if results is None else None
         out_ev: List[Optional[torch.cuda.Event]] = [None] * DEPTH
         ftle_dev = [torch.empty(nmax, dtype=torch.float64, device=dev) for _ in range(DEPTH)]
-        kernel_ev = []
+        # events made once and reused by window i % DEPTH: a slot is recorded again only
+        # after its previous window was emitted (its kernel time read there)
+        kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(DEPTH)]
+        oev = [torch.cuda.Event() for _ in range(DEPTH)]
+        fused = [0, 0.0]  # windows timed, their kernel milliseconds
         descs = {}  # one window descriptor per particle file, re-pointed per window
+        plans = {}  # host slot -> device copy plans (io.slot_to_device)
 
         def host_out(i, n):
             return results[i, :n] if results is not None else out_pin[i % DEPTH][:n]
@@ -194,19 +200,22 @@ class SlidingWindowRunner:
                 if node_used[j % 2] is not None:  # a step of the first window still reads it
                     copy.wait_event(node_used[j % 2])
                 # the file's data ranges to the device, reordered there into node order
-                buf = io.slot_to_device(host.bufs[slot], layout, dim, nodes, raw[j % 2], nb)
-                ev = torch.cuda.Event()
-                ev.record(copy)
-                host.release_after(slot, ev)
+                buf = io.slot_to_device(host.bufs[slot], layout, dim, nodes, raw[j % 2], nb,
+                                        cache=plans)
                 _lib.call("ftle_pack_snapshots", dim, nodes, 1, 0, buf.data_ptr(), _lib.F64,
                           ring_dev.data_ptr() + (j % R) * block, stream_ptr(copy))
                 e = torch.cuda.Event()
-                e.record(copy)
+                e.record(copy)  # the slot's copy and the packing are done
+                host.release_after(slot, e)
                 packed[j] = e
 
         def emit(i):
             _, pf, _, ident = wins[i]
             out_ev[i % DEPTH].synchronize()
+            if i >= start:  # a fused window: its kernel time, before the events are reused
+                k0, k1 = kev[i % DEPTH]
+                fused[0] += 1
+                fused[1] += k0.elapsed_time(k1)
             arr = host_out(i, N[pf]).numpy()
             if results is None:
                 arr = arr.copy()  # the ring slot is reused
@@ -244,48 +253,40 @@ class SlidingWindowRunner:
             d.record(comp)
             done[0] = d
             host_out(0, N[pf]).copy_(f, non_blocking=True)
-            e = torch.cuda.Event()
-            e.record(comp)
-            out_ev[0] = e
+            oev[0].record(comp)
+            out_ev[0] = oev[0]
 
+        start = 1 if self.first_window_per_step and p <= n else 0
         try:
-            start = 0
-            if self.first_window_per_step and p <= n:
+            if start:
                 first_window_by_steps()
-                start = 1
                 if p < n:
                     stage(p)
             else:
                 for j in range(min(p, n)):
                     stage(j)
             t_first = time.perf_counter()
+            sp = stream_ptr(comp)
             for i in range(start, W):
                 _, pf, _, _ = wins[i]
                 comp.wait_event(packed[i + p - 1])  # in order: every earlier block is packed too
-                pos = seeds[pf].positions.clone()
                 f = ftle_dev[i % DEPTH][:N[pf]]
                 w = descs.get(pf)
-                if w is None:
+                if w is None:  # the seeds are read, never written (no per-window copy)
                     w = descs[pf] = window_descriptor(
-                        series, pos, f, integrator=self.integrator, time_mode="hold", h=dt,
-                        num_steps=p, map_period=(p - 1) * abs(dt), first_snapshot=i % R,
-                        snapshot_dt=dt)
+                        series, seeds[pf].positions, f, integrator=self.integrator,
+                        time_mode="hold", h=dt, num_steps=p, map_period=(p - 1) * abs(dt),
+                        first_snapshot=i % R, snapshot_dt=dt, keep_positions=True)
                 w.first_snapshot = i % R
-                w.positions = pos.data_ptr()
                 w.ftle = f.data_ptr()
-                k0 = torch.cuda.Event(enable_timing=True)
-                k1 = torch.cuda.Event(enable_timing=True)
+                k0, k1 = kev[i % DEPTH]
                 k0.record(comp)
-                _lib.call("ftle_window_run_f64", w, stream_ptr(comp))
+                _lib.call("ftle_window_run_f64", w, sp)
                 k1.record(comp)
-                kernel_ev.append((k0, k1))
-                d = torch.cuda.Event()
-                d.record(comp)
-                done[i] = d
+                done[i] = k1
                 host_out(i, N[pf]).copy_(f, non_blocking=True)
-                e = torch.cuda.Event()
-                e.record(comp)
-                out_ev[i % DEPTH] = e
+                oev[i % DEPTH].record(comp)
+                out_ev[i % DEPTH] = oev[i % DEPTH]
                 if i + p < n:
                     stage(i + p)  # overlaps the windows in flight
                 if i >= DEPTH - 1:
@@ -300,12 +301,12 @@ class SlidingWindowRunner:
         finally:
             pool.shutdown(wait=True)
         torch.cuda.synchronize()
-        fused_ms = sum(a.elapsed_time(b) for a, b in kernel_ev)
+        nf, fused_ms = fused
         self.stats = {"seconds": time.perf_counter() - t_start,
                       "first_window_s": t_first - t_start,
-                      "fused_windows": len(kernel_ev), "fused_kernel_ms": fused_ms,
+                      "fused_windows": nf, "fused_kernel_ms": fused_ms,
                       # every window's kernel time, the first one counted at the fused rate
-                      "kernel_ms": fused_ms * W / len(kernel_ev) if kernel_ev else 0.0,
+                      "kernel_ms": fused_ms * W / nf if nf else 0.0,
                       "windows": W, "device_ring_snapshots": R,
                       "host_ring_buffers": len(host.bufs)}
         return None if self.writer is not None else fields
