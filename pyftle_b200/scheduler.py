@@ -35,9 +35,9 @@ class SlidingWindowRunner:
     def __init__(self, snapshot_files: List[str], coordinate_files: List[str],
                  particle_files: List[str], snapshot_timestep: float, flow_map_period: float,
                  grid_shape: tuple, integrator_name: str = "rk4", writer=None,
-                 precision: str = "fp64", periodic_space: bool = False, workers: int = 8,
+                 precision: str = "fp64", periodic_space: bool = False, workers: int = 4,
                  streaming: bool = True, device_depth: int = 2,
-                 first_window_per_step: bool = True):
+                 head_per_step: bool = True, head_windows: Optional[int] = None):
         self.snapshot_files = list(snapshot_files)
         self.coordinate_files = list(coordinate_files)
         self.particle_files = list(particle_files)
@@ -51,7 +51,8 @@ class SlidingWindowRunner:
         self.workers = workers
         self.streaming = bool(streaming)
         self.device_depth = max(1, int(device_depth))
-        self.first_window_per_step = bool(first_window_per_step)
+        self.head_per_step = bool(head_per_step)
+        self.head_windows = head_windows
         self.stats: dict = {}
         if self.timestep < 0:  # backward time: reverse the file order
             self.snapshot_files.reverse()
@@ -118,10 +119,14 @@ class SlidingWindowRunner:
         snapshot i + p (needed by window i + 1) then run while window i's kernel runs,
         a ring block is overwritten only after the last window reading it finished,
         and window i - 1's FTLE is copied back and emitted on the host meanwhile.
-        With ``first_window_per_step`` window 0 does not wait for its p files: it is
-        advanced one launch per step (``ftle_grid_step``) as each snapshot arrives and
-        its FTLE taken from the final positions (``ftle_from_positions``) -- the fused
-        kernel's bits (same step arithmetic, same FTLE device function).
+        With ``head_per_step`` the first windows (``head_windows`` of them, default
+        (p + 1) // 2, at most the p that start before window 0's last file arrives,
+        while they share window 0's particle file) do not wait for their p files: when snapshot j arrives, every such window w with
+        w <= j < w + p takes its step j - w -- all of them on snapshot j (HOLD) -- in
+        one ``ftle_grid_step`` launch over their adjacent position blocks, and a window's
+        FTLE is taken from its final positions (``ftle_from_positions``): the fused
+        kernel's bits (same step arithmetic, same FTLE device function), with the GPU
+        busy while the first files are still being read.
         Device memory holds p + device_depth snapshots instead of all n.
         """
         import time
@@ -146,6 +151,7 @@ class SlidingWindowRunner:
         node_bufs = [torch.empty((dim, nodes), dtype=torch.float64, device=dev)
                      for _ in range(2)]
         node_used: List[Optional[torch.cuda.Event]] = [None, None]
+        ev_node = [torch.cuda.Event(), torch.cuda.Event()]
         series = _RingSeries(grid, ring_dev, R)
         comp = torch.cuda.current_stream(dev)
         copy = torch.cuda.Stream(device=dev)
@@ -178,12 +184,26 @@ class SlidingWindowRunner:
         kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(DEPTH)]
         oev = [torch.cuda.Event() for _ in range(DEPTH)]
+        ev_ftle = [torch.cuda.Event() for _ in range(DEPTH)]
         fused = [0, 0.0]  # windows timed, their kernel milliseconds
         descs = {}  # one window descriptor per particle file, re-pointed per window
         plans = {}  # host slot -> device copy plans (io.slot_to_device)
 
         def host_out(i, n):
             return results[i, :n] if results is not None else out_pin[i % DEPTH][:n]
+
+        # FTLE fields go back on a stream of their own, so the compute stream runs window
+        # after window without the copies between them
+        back = torch.cuda.Stream(device=dev)
+
+        def fetch(i, f, after):
+            """Window i's FTLE `f` to host memory once `after` (an event on the compute
+            stream) has passed; out_ev[i % DEPTH] marks the copy's end."""
+            back.wait_event(after)
+            with torch.cuda.stream(back):
+                host_out(i, f.shape[0]).copy_(f, non_blocking=True)
+            oev[i % DEPTH].record(back)
+            out_ev[i % DEPTH] = oev[i % DEPTH]
         fields = []
 
         pool = ThreadPoolExecutor(max_workers=max(1, self.workers))
@@ -194,8 +214,9 @@ class SlidingWindowRunner:
             slot, layout = futures[j].result()
             with torch.cuda.stream(copy):
                 prev = j - R  # the snapshot that last used ring block j % R
-                if prev >= 0:
-                    copy.wait_event(done[min(prev, W - 1)])  # last window that read it
+                last = min(prev, W - 1)  # the last window that read it from the ring
+                if prev >= 0 and done[last] is not None:  # (head windows do not read it)
+                    copy.wait_event(done[last])
                 nb = node_bufs[j % 2]
                 if node_used[j % 2] is not None:  # a step of the first window still reads it
                     copy.wait_event(node_used[j % 2])
@@ -225,43 +246,64 @@ class SlidingWindowRunner:
             else:
                 fields.append(arr)
 
-        def first_window_by_steps():
-            """Window 0 advanced one launch per step (ftle_grid_step) as its snapshots
-            arrive, then its FTLE from the final positions: the fused kernel's bits
-            (same step arithmetic, same FTLE device function), with the window's
-            compute overlapping its own file reads."""
+        # head windows: a prefix of windows sharing window 0's particle file, at most
+        # head_windows (default: half a window length, which balances the per-step
+        # work against the reading of the first files)
+        H = 0
+        if self.head_per_step and p <= n:
+            cap = (p + 1) // 2 if self.head_windows is None else int(self.head_windows)
+            cap = max(1, min(W, p, cap))
+            while H < cap and wins[H][1] == wins[0][1]:
+                H += 1
+
+        def head_windows_by_steps():
+            """Windows 0 .. H-1 advanced one launch per arriving snapshot (see above)."""
             _, pf, _, _ = wins[0]
             part = seeds[pf]
-            pos = part.positions.clone()
+            m = part.positions.shape[0]  # particles per window
+            big = torch.empty((H,) + tuple(part.positions.shape), dtype=torch.float64,
+                              device=dev)
             code = _lib.INTEGRATOR_CODES[self.integrator]
-            hist = torch.empty_like(pos) if self.integrator == "ab2" else None
-            for j in range(p):
+            hist = torch.empty_like(big) if self.integrator == "ab2" else None
+            idl = part.initial_deltas()
+            T = float((p - 1) * abs(dt))
+            gabi = grid.to_abi()
+            sp = stream_ptr(comp)
+
+            def step(lo, hi, j, valid):  # windows lo..hi take their step on snapshot j
+                _lib.call("ftle_grid_step", gabi, node_bufs[j % 2].data_ptr(), code, float(dt),
+                          big[lo].data_ptr(), (hi - lo + 1) * m,
+                          hist[lo].data_ptr() if hist is not None else None, int(valid), sp)
+
+            for j in range(H + p - 1):
                 stage(j)
                 comp.wait_event(packed[j])
-                _lib.call("ftle_grid_step", grid.to_abi(), node_bufs[j % 2].data_ptr(), code,
-                          float(dt), pos.data_ptr(), pos.shape[0],
-                          hist.data_ptr() if hist is not None else None, int(j > 0),
-                          stream_ptr(comp))
-                e = torch.cuda.Event()
-                e.record(comp)
-                node_used[j % 2] = e
-            f = ftle_dev[0][:N[pf]]
-            idl = part.initial_deltas()
-            _lib.call("ftle_from_positions", dim, pos.data_ptr(), idl.data_ptr(), N[pf],
-                      float((p - 1) * abs(dt)), f.data_ptr(), stream_ptr(comp))
-            d = torch.cuda.Event()
-            d.record(comp)
-            done[0] = d
-            host_out(0, N[pf]).copy_(f, non_blocking=True)
-            oev[0].record(comp)
-            out_ev[0] = oev[0]
+                lo, hi = max(0, j - p + 1), min(j, H - 1)
+                if j < H:  # window j starts: its seeds, then its first step
+                    big[j].copy_(part.positions)
+                    if hist is not None:
+                        step(j, j, j, False)  # AB2's first step is Euler
+                        hi = j - 1
+                if lo <= hi:
+                    step(lo, hi, j, True)
+                node_used[j % 2] = ev_node[j % 2]
+                ev_node[j % 2].record(comp)
+                w = j - p + 1  # the window whose last snapshot is j
+                if w >= 0:
+                    f = ftle_dev[w % DEPTH][:N[pf]]
+                    _lib.call("ftle_from_positions", dim, big[w].data_ptr(), idl.data_ptr(),
+                              N[pf], T, f.data_ptr(), sp)
+                    ev_ftle[w % DEPTH].record(comp)
+                    fetch(w, f, ev_ftle[w % DEPTH])
+                    if w >= DEPTH - 1:
+                        emit(w - (DEPTH - 1))
 
-        start = 1 if self.first_window_per_step and p <= n else 0
+        start = H
         try:
             if start:
-                first_window_by_steps()
-                if p < n:
-                    stage(p)
+                head_windows_by_steps()
+                if H + p - 1 < n:
+                    stage(H + p - 1)  # the last snapshot of window H
             else:
                 for j in range(min(p, n)):
                     stage(j)
@@ -284,9 +326,7 @@ class SlidingWindowRunner:
                 _lib.call("ftle_window_run_f64", w, sp)
                 k1.record(comp)
                 done[i] = k1
-                host_out(i, N[pf]).copy_(f, non_blocking=True)
-                oev[i % DEPTH].record(comp)
-                out_ev[i % DEPTH] = oev[i % DEPTH]
+                fetch(i, f, k1)
                 if i + p < n:
                     stage(i + p)  # overlaps the windows in flight
                 if i >= DEPTH - 1:
@@ -303,7 +343,7 @@ class SlidingWindowRunner:
         torch.cuda.synchronize()
         nf, fused_ms = fused
         self.stats = {"seconds": time.perf_counter() - t_start,
-                      "first_window_s": t_first - t_start,
+                      "head_s": t_first - t_start, "head_windows": H,
                       "fused_windows": nf, "fused_kernel_ms": fused_ms,
                       # every window's kernel time, the first one counted at the fused rate
                       "kernel_ms": fused_ms * W / nf if nf else 0.0,

@@ -102,9 +102,9 @@ def test_streaming_windows_equal_resident_series(golden, tmp_path, direction):
     kw = dict(flow_map_period=2 * abs(dt), grid_shape=shape, workers=2)
     resident = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **kw)
     b = resident.run()
-    for by_steps in (True, False):  # the first window by per-step launches, or fused
+    for by_steps in (True, False):  # the head windows by per-step launches, or all fused
         streamed = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, device_depth=1,
-                                       first_window_per_step=by_steps, **kw)
+                                       head_per_step=by_steps, **kw)
         a = streamed.run()
         assert streamed.stats["device_ring_snapshots"] == streamed.window_length + 1
         assert len(a) == len(b) == len(files) - streamed.window_length + 1
@@ -113,13 +113,52 @@ def test_streaming_windows_equal_resident_series(golden, tmp_path, direction):
 
 
 @pytest.mark.parametrize("integrator", ["euler", "ab2"])
-def test_streaming_first_window_steps_other_integrators(golden, tmp_path, integrator):
+def test_streaming_head_windows_other_integrators(golden, tmp_path, integrator):
     d = golden("windows_2d.npz")
     shape = tuple(d["shape"])
     files, cf, pf = _write_case(tmp_path, d)
     dt = float(d["dt"])
     kw = dict(flow_map_period=3 * dt, grid_shape=shape, workers=2, integrator_name=integrator)
     b = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **kw).run()
-    a = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, **kw).run()
+    for head in (None, 1, 4):  # the default (p + 1) // 2, one, all p = 4 head windows
+        r = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, head_windows=head, **kw)
+        a = r.run()
+        H = (r.window_length + 1) // 2 if head is None else head
+        assert r.stats["head_windows"] == H  # then fused windows follow
+        assert r.stats["fused_windows"] == len(b) - H
+        for x, y in zip(a, b):
+            np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("integrator", ["rk4", "ab2"])
+def test_streaming_head_windows_edge_cases(golden, tmp_path, integrator):
+    """Every window a head window (no fused window at all), and windows that alternate
+    between two particle files (the head stops at the first window with another file)."""
+    d = golden("windows_2d.npz")
+    shape = tuple(d["shape"])
+    files, cf, pf = _write_case(tmp_path, d)
+    dt = float(d["dt"])
+    kw = dict(grid_shape=shape, workers=2, integrator_name=integrator)
+    long = dict(kw, flow_map_period=6 * dt)  # p = 7: windows 0..4 all start before file 6
+    b = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **long).run()
+    r = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, head_windows=7, **long)
+    a = r.run()
+    assert r.stats["head_windows"] == len(b) and r.stats["fused_windows"] == 0
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    # a second particle file: the first half of the first file's groups, in role blocks
+    pos = d["positions"]
+    N = pos.shape[0] // 4
+    M = N // 2
+    pf2 = tmp_path / "seeds2.mat"
+    savemat(pf2, {"left": pos[:M], "right": pos[N:N + M], "top": pos[2 * N:2 * N + M],
+                  "bottom": pos[3 * N:3 * N + M]})
+    two = dict(kw, flow_map_period=2 * dt)
+    b = SlidingWindowRunner(files, [cf], [pf, str(pf2)], dt, streaming=False, **two).run()
+    r = SlidingWindowRunner(files, [cf], [pf, str(pf2)], dt, streaming=True, **two)
+    a = r.run()
+    assert r.stats["head_windows"] == 1
+    assert [x.shape[0] for x in a] == [x.shape[0] for x in b]
+    assert {x.shape[0] for x in a} == {N, M}
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
