@@ -37,6 +37,8 @@ class EngineOptions:
     periodic_time: bool = False  # snapshot index wraps modulo the series length
     chunk_steps: Optional[int] = None  # mixed path: steps per launch (None: one launch)
     sort_every: int = 1          # mixed chunked path: cell-sort the groups every n chunks
+    judge_tol: Optional[float] = None  # mixed path: FP64 judge on a sample, re-advect above
+    judge_stride: int = 100      # the judge's sample: every n-th group (1% by default)
 
 
 class SnapshotSeries:

@@ -511,3 +511,53 @@ def test_fx16_codes_decode_to_the_nearest_level(dim):
         step = scale[c] * np.where(q[:, :, c] < 32768, 1.0 / 65536.0, 1.0 / 32768.0)
         assert np.all(np.abs(u - v) <= 0.5 * step * (1 + 1e-6) + 1e-6 * np.abs(v)), c
         assert (scale[c] * (2.0 - 2.0 ** -15) + offset[c]) >= v.max() - 1e-6
+
+
+# ---------------------------------------------------------------------------
+# FP64 judge of a mixed-precision window (FTLESolver, EngineOptions.judge_tol)
+# ---------------------------------------------------------------------------
+
+def _abc_judge_case():
+    n = 32
+    ax = flows.periodic_axis(n)
+    S = 16
+    dt = 2 * math.pi / S
+    snaps = flows.abc_snapshots(ax, ax, ax, np.arange(S) * dt)
+    pts = flows.grid_points_3d(ax, ax, ax)
+    cents = np.random.default_rng(21).uniform(0, 2 * math.pi, (1500, 3))
+    pos = flows.seeds_3d(cents, 1e-3)
+    kw = dict(h=0.02, num_steps=150, snapshot_dt=dt, periodic_space=True, periodic_time=True)
+    return snaps, pts, pos, (n, n, n), kw
+
+
+def _solve(snaps, pts, pos, shape, kw, **opts):
+    src = BlendedSnapshotSource(snaps, pts, pos, shape, **kw)
+    solver = FTLESolver(src, create_integrator("rk4", create_interpolator("grid", shape)),
+                        options=EngineOptions(**opts))
+    f = solver.run()
+    return f, solver.particles.positions.cpu().numpy(), solver
+
+
+def test_judge_readvects_a_window_above_tolerance():
+    """BF16 storage misses a tight tolerance: the window comes back as the plain FP64
+    path's bits (FTLE and final positions), and the judge reports the sampled error."""
+    snaps, pts, pos, shape, kw = _abc_judge_case()
+    f64, p64, _ = _solve(snaps, pts, pos, shape, kw)
+    fbf, _, _ = _solve(snaps, pts, pos, shape, kw, precision="bf16")
+    f, p, solver = _solve(snaps, pts, pos, shape, kw, precision="bf16", judge_tol=1e-6,
+                          judge_stride=10)
+    sel = np.arange(0, f64.size, 10)
+    assert solver.judge["readvected"] and solver.judge["sample_groups"] == sel.size
+    assert solver.judge["error"] == pytest.approx(rel_l2(fbf[sel], f64[sel]), rel=1e-12)
+    np.testing.assert_array_equal(f, f64)
+    np.testing.assert_array_equal(p, p64)
+
+
+def test_judge_keeps_a_window_within_tolerance():
+    snaps, pts, pos, shape, kw = _abc_judge_case()
+    fx, px, _ = _solve(snaps, pts, pos, shape, kw, precision="fx16", chunk_steps=40)
+    f, p, solver = _solve(snaps, pts, pos, shape, kw, precision="fx16", chunk_steps=40,
+                          judge_tol=1e-3)
+    assert not solver.judge["readvected"] and 0 < solver.judge["error"] <= 1e-3
+    np.testing.assert_array_equal(f, fx)
+    np.testing.assert_array_equal(p, px)
