@@ -72,8 +72,9 @@ def parse_args():
     p.add_argument("--chunk-steps", type=int, default=50,
                    help="mixed path: steps per launch between cell sorts (0: one launch)")
     p.add_argument("--sort-every", type=int, default=1)
-    p.add_argument("--plain-fraction", type=float, default=0.125,
-                   help="share of the groups the plain FP64 leg advects")
+    p.add_argument("--plain-fraction", type=float, default=1.0,
+                   help="share of the groups the plain FP64 leg advects (the first ones; "
+                        "1.0: the whole field, the same work as the chosen path)")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -388,7 +389,7 @@ def run_ours(args):
     value = world * particle_steps * args.steps / (elapsed_ms / 1e3)
     ftle_chosen = ftle.clone()
 
-    # --- plain FP64 leg (same groups, a slice of them) + FTLE error ----------
+    # --- plain FP64 leg (the same groups: all of them by default) + FTLE error -
     plain = None
     if not args.no_plain and args.precision != "fp64":
         m = max(1, int(N * args.plain_fraction))
