@@ -111,3 +111,40 @@ def test_direct_mat_reader_matches_loadmat(tmp_path):
     fm = tmp_path / "mixed.mat"
     savemat(fm, {"velocity_x": rng.random((2, 3)), "velocity_y": rng.random((3, 2))})
     assert io._raw_components(fm, "velocity") is None
+
+
+def test_slot_copy_plan_cache_gives_each_files_values(tmp_path):
+    """The copy plan cached per (slot, scratch, output, layout) serves later files of the
+    same layout in the same slot: each comes out in the reference's node order (what
+    read_velocity returns), with or without the cache (CPU tensors stand in for the
+    device here; the plan is the same tensor views either way)."""
+    import torch
+
+    ny, nx = 6, 9
+    rng = np.random.default_rng(3)
+    files = []
+    for i in range(3):
+        f = tmp_path / f"v{i}.mat"
+        savemat(f, {"velocity_x": rng.random((ny, nx)), "velocity_y": rng.random((ny, nx))})
+        files.append(str(f))
+    size = max(len(open(f, "rb").read()) for f in files)
+    slot = torch.zeros(size + 64, dtype=torch.uint8)
+    raw = torch.empty((2, nx * ny), dtype=torch.float64)
+    kept = torch.empty((2, nx * ny), dtype=torch.float64)  # the cached path's output
+    cache = {}
+    for f in files:
+        data = open(f, "rb").read()
+        slot.zero_()
+        slot[:len(data)] = torch.frombuffer(bytearray(data), dtype=torch.uint8)
+        lay = io._component_layout(
+            io._mat_parse(memoryview(slot.numpy())[:len(data)], ["velocity_x", "velocity_y"],
+                          ["velocity_z"]), "velocity")
+        assert lay is not None
+        want = io.read_velocity(f)
+        got = io.slot_to_device(slot, lay, 2, nx * ny, raw,
+                                torch.empty((2, nx * ny), dtype=torch.float64))
+        np.testing.assert_array_equal(got.numpy(), want)
+        got = io.slot_to_device(slot, lay, 2, nx * ny, raw, kept, cache=cache)
+        assert got.data_ptr() == kept.data_ptr()
+        np.testing.assert_array_equal(kept.numpy(), want)
+    assert len(cache) == 1  # one slot, one scratch, one output, one layout: one plan
