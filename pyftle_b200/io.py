@@ -358,19 +358,6 @@ def slot_to_device(slot_buf: torch.Tensor, layout, dim: int, nodes: int, raw: to
     return out
 
 
-def to_node_order(raw: torch.Tensor, order, out: torch.Tensor) -> torch.Tensor:
-    """``out`` (dim, nodes) <- the device copy ``raw`` of a slot in node order (the
-    transposition of column-major (rows, cols) components runs on the device)."""
-    if order is None:
-        if out.data_ptr() != raw.data_ptr():
-            out.copy_(raw)
-        return out
-    rows, cols = order
-    dim = raw.shape[0]
-    out.view(dim, rows, cols).copy_(raw.view(dim, cols, rows).transpose(1, 2))
-    return out
-
-
 def load_snapshots(files: Sequence[str], dim: int, nodes: int, workers: int = 8,
                    device=None) -> torch.Tensor:
     """Read velocity files in parallel into a (S, dim, nodes) float64 device tensor.
