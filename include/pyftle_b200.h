@@ -167,7 +167,7 @@ int ftle_pack_snapshots(int32_t dim, int64_t nodes, int32_t num_snapshots,
  * pyFTLE's positions; FTLE within 1e-10 relative. */
 int ftle_window_run_f64(const ftle_window *w, void *stream);
 
-/* Mixed-precision window (storage FTLE_F16, FTLE_BF16 or FTLE_FX15): FP32 advection of
+/* Mixed-precision window (storage FTLE_F16, FTLE_BF16, FTLE_FX15 or FTLE_FX16): FP32 advection of
  * each group as an FP64 centroid plus FP32 neighbour offsets (split
  * representation), FP64 Jacobian -> Cauchy-Green -> lambda_max.  Writes
  * FP64 positions = centroid + offset. */
