@@ -653,23 +653,50 @@ __device__ __forceinline__ void eval_group(const MixK &m, const Header16 &hd,
   if constexpr (DIM == 2) {
     if (!__any_sync(0xffffffffu, off != 0u)) return;
   }
-  // pass 2: queue the off-cell neighbours of the whole warp
-  const int cnt = __popc(off);
-  int incl = cnt;
+  // pass 2: queue the off-cell neighbours of the whole warp.  2D queues them neighbour
+  // by neighbour (every lane's neighbour 0, then every lane's neighbour 1, ...: the
+  // same neighbour of Morton-adjacent groups mostly lies in the same cell, so a gather
+  // pass's loads share lines; measured +2.3 % on the 2D batch), 3D lane by lane (the
+  // neighbour order measured 0.5 % slower there).  Same items either way, same bits.
+  int total;
+  if constexpr (DIM == 2) {
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned bal[K];
+    int start[K];
+    total = 0;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  if (total == 0) return;  // warp-uniform
-  __syncwarp();  // every lane has read its slots of the previous stage
-  int pos = incl - cnt;
+    for (int k = 0; k < K; ++k) {
+      bal[k] = __ballot_sync(0xffffffffu, (off >> k) & 1u);
+      start[k] = total;
+      total += __popc(bal[k]);
+    }
+    if (total == 0) return;  // warp-uniform
+    __syncwarp();  // every lane has read its slots of the previous stage
 #pragma unroll
-  for (int a = 0; a < DIM; ++a) wq.ci[a][lane] = ci[a];
+    for (int a = 0; a < DIM; ++a) wq.ci[a][lane] = ci[a];
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    if (off & (1u << k)) wq.dst[pos++] = k * DIM * kBlock + (int)threadIdx.x;
+    for (int k = 0; k < K; ++k) {
+      if (off & (1u << k))
+        wq.dst[start[k] + __popc(bal[k] & lt)] = k * DIM * kBlock + (int)threadIdx.x;
+    }
+  } else {
+    const int cnt = __popc(off);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) return;  // warp-uniform
+    __syncwarp();  // every lane has read its slots of the previous stage
+    int pos = incl - cnt;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) wq.ci[a][lane] = ci[a];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (off & (1u << k)) wq.dst[pos++] = k * DIM * kBlock + (int)threadIdx.x;
+    }
   }
   __syncwarp();
   // pass 3: 32 queued gathers at a time (a group whose centroid is not finite queues
