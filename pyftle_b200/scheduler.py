@@ -31,6 +31,10 @@ from pyftle_b200.particles import NeighboringParticles
 from pyftle_b200.window import SnapshotSeries, run_window
 
 
+# device memory the head windows' position blocks may take (see _run_streaming)
+HEAD_BYTES = 1 << 30
+
+
 class SlidingWindowRunner:
     def __init__(self, snapshot_files: List[str], coordinate_files: List[str],
                  particle_files: List[str], snapshot_timestep: float, flow_map_period: float,
@@ -121,7 +125,8 @@ class SlidingWindowRunner:
         and window i - 1's FTLE is copied back and emitted on the host meanwhile.
         With ``head_per_step`` the first windows (``head_windows`` of them, default
         (p + 1) // 2, at most the p that start before window 0's last file arrives,
-        while they share window 0's particle file) do not wait for their p files: when snapshot j arrives, every such window w with
+        while they share window 0's particle file, and at least one but no more than
+        whose positions fit in ``HEAD_BYTES``) do not wait for their p files: when snapshot j arrives, every such window w with
         w <= j < w + p takes its step j - w -- all of them on snapshot j (HOLD) -- in
         one ``ftle_grid_step`` launch over their adjacent position blocks, and a window's
         FTLE is taken from its final positions (``ftle_from_positions``): the fused
@@ -248,11 +253,13 @@ class SlidingWindowRunner:
 
         # head windows: a prefix of windows sharing window 0's particle file, at most
         # head_windows (default: half a window length, which balances the per-step
-        # work against the reading of the first files)
+        # work against the reading of the first files), and no more than keep their
+        # positions (and AB2 histories) within HEAD_BYTES of device memory
         H = 0
         if self.head_per_step and p <= n:
             cap = (p + 1) // 2 if self.head_windows is None else int(self.head_windows)
-            cap = max(1, min(W, p, cap))
+            per = seeds[wins[0][1]].positions.numel() * 8 * (2 if self.integrator == "ab2" else 1)
+            cap = max(1, min(W, p, cap, HEAD_BYTES // max(per, 1)))
             while H < cap and wins[H][1] == wins[0][1]:
                 H += 1
 

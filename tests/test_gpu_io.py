@@ -162,3 +162,22 @@ def test_streaming_head_windows_edge_cases(golden, tmp_path, integrator):
     assert {x.shape[0] for x in a} == {N, M}
     for x, y in zip(a, b):
         np.testing.assert_array_equal(x, y)
+
+
+def test_streaming_head_windows_capped_by_memory(golden, tmp_path, monkeypatch):
+    """The head windows' position blocks stay within the runner's memory budget: with a
+    budget of two windows' positions only two windows are head windows (same bits)."""
+    from pyftle_b200 import scheduler
+
+    d = golden("windows_2d.npz")
+    shape = tuple(d["shape"])
+    files, cf, pf = _write_case(tmp_path, d)
+    dt = float(d["dt"])
+    kw = dict(flow_map_period=5 * dt, grid_shape=shape, workers=2)
+    b = SlidingWindowRunner(files, [cf], [pf], dt, streaming=False, **kw).run()
+    monkeypatch.setattr(scheduler, "HEAD_BYTES", d["positions"].size * 8 * 2)
+    r = SlidingWindowRunner(files, [cf], [pf], dt, streaming=True, head_windows=6, **kw)
+    a = r.run()
+    assert r.stats["head_windows"] == 2
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
