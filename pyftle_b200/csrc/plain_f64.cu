@@ -614,8 +614,14 @@ __global__ void grid_interpolate_kernel(const GridK g, const double *__restrict_
 template <int DIM, int INTEG>
 __global__ void grid_step_kernel(const GridK g, const double *__restrict__ snap, double h,
                                  double *pos, long long m, double *hist, int hist_valid) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
-       i += (long long)gridDim.x * blockDim.x) {
+  // When m = K*N (role-blocked neighbour groups), work item j takes role j mod K of
+  // group j / K, so a warp holds every neighbour of a few groups and their gathers share
+  // cells; each particle is still advected once, by the same arithmetic.
+  constexpr int K = 2 * DIM;
+  const long long ng = (m % K == 0) ? m / K : 0;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < m;
+       j += (long long)gridDim.x * blockDim.x) {
+    const long long i = ng ? (j % K) * ng + j / K : j;
     double x[DIM];
 #pragma unroll
     for (int a = 0; a < DIM; ++a) x[a] = pos[i * DIM + a];
