@@ -119,20 +119,25 @@ class SlidingWindowRunner:
         into a device ring of ``p + device_depth`` snapshot blocks, which the kernel
         addresses modulo the ring length (``periodic_time`` with ``first_snapshot`` =
         window index mod ring length; HOLD reads one snapshot per step).  Window i is
-        launched as soon as its p snapshots are packed; the read, copy and packing of
-        snapshot i + p (needed by window i + 1) then run while window i's kernel runs,
-        a ring block is overwritten only after the last window reading it finished,
-        and window i - 1's FTLE is copied back and emitted on the host meanwhile.
-        With ``head_per_step`` the first windows (``head_windows`` of them, default
-        (p + 1) // 2, at most the p that start before window 0's last file arrives,
-        while they share window 0's particle file, and at least one but no more than
-        whose positions fit in ``HEAD_BYTES``) do not wait for their p files: when snapshot j arrives, every such window w with
-        w <= j < w + p takes its step j - w -- all of them on snapshot j (HOLD) -- in
-        one ``ftle_grid_step`` launch over their adjacent position blocks, and a window's
-        FTLE is taken from its final positions (``ftle_from_positions``): the fused
-        kernel's bits (same step arithmetic, same FTLE device function), with the GPU
-        busy while the first files are still being read.
-        Device memory holds p + device_depth snapshots instead of all n.
+        launched as soon as its p snapshots are packed, reading its particle file's
+        seeds without writing them; the read, copy and packing of snapshot i + p
+        (needed by window i + 1) then run while window i's kernel runs, and a ring block
+        is overwritten only after the last window reading it finished.  Up to DEPTH
+        windows are in flight: each window's FTLE goes back to host memory on a stream
+        of its own (one pinned array for all windows when no writer is given) and is
+        emitted while the next windows run.
+
+        With ``head_per_step`` the first windows -- ``head_windows`` of them (default
+        (p + 1) // 2), at most the p that start before window 0's last file arrives,
+        only while they share window 0's particle file, and no more than fit their
+        positions in ``HEAD_BYTES`` (at least one) -- do not wait for their p files:
+        when snapshot j arrives, every such window w with w <= j < w + p takes its step
+        j - w, all of them on snapshot j (HOLD), in one ``ftle_grid_step`` launch over
+        their adjacent position blocks, and a window's FTLE is taken from its final
+        positions (``ftle_from_positions``): the fused kernel's bits (same step
+        arithmetic, same FTLE device function), with the GPU busy while the first files
+        are still being read.  Device memory holds p + device_depth snapshots instead of
+        all n.
         """
         import time
         from concurrent.futures import ThreadPoolExecutor

@@ -32,13 +32,17 @@ from pyftle_b200.interpolate import GridSpec
 class EngineOptions:
     """Knobs of the fused path (no reference counterpart)."""
 
-    precision: str = "fp64"      # "fp64" (plain, reference arithmetic) | "fx15" | "fx16" | "fp16" | "bf16"
+    # "fp64" (plain, the reference's arithmetic) | "fx16" | "fx15" | "fp16" | "bf16"
+    precision: str = "fp64"
     time_mode: str = "hold"      # "hold" (reference) | "blend"
     periodic_time: bool = False  # snapshot index wraps modulo the series length
     chunk_steps: Optional[int] = None  # mixed path: steps per launch (None: one launch)
     sort_every: int = 1          # mixed chunked path: cell-sort the groups every n chunks
-    judge_tol: Optional[float] = None  # mixed path: FP64 judge on a sample, re-advect above
-    judge_stride: int = 100      # the judge's sample: every n-th group (1% by default)
+    # mixed path: the plain FP64 kernel judges the field on every judge_stride-th group
+    # (1 % by default) and re-advects the window in FP64 when the sampled FTLE error is
+    # above judge_tol (FTLESolver keeps a copy of the seeds for that)
+    judge_tol: Optional[float] = None
+    judge_stride: int = 100
 
 
 class SnapshotSeries:
