@@ -231,9 +231,9 @@ class WindowBatch:
     def run_judged(self, series64: SnapshotSeries, *, tol: float = 1e-3,
                    sample_stride: int = 100, fallback: bool = True,
                    schedule: Optional[Schedule] = None) -> "JudgeReport":
-        """Run the batch, then judge every window against plain FP64 RK4 on a sample
-        of its groups and re-advect in FP64 every window whose sampled error exceeds
-        ``tol``.
+        """Run the batch, then judge every window against the plain FP64 path (the
+        batch's integrator and time mode) on a sample of its groups and re-advect in
+        FP64 every window whose sampled error exceeds ``tol``.
 
         The sample of window i is every ``sample_stride``-th group starting at group
         ``i mod sample_stride`` (1% at the default), advected by the plain FP64
@@ -248,8 +248,11 @@ class WindowBatch:
         """
         if series64.storage != _lib.F64:
             raise ValueError("series64 must hold the snapshots as \"fp64\"")
-        if series64.grid.shape != self.series.grid.shape:
-            raise ValueError("series64 must cover the batch's grid")
+        if (series64.grid.shape != self.series.grid.shape
+                or series64.num_snapshots != self.series.num_snapshots
+                or series64.periodic_time != self.series.periodic_time):
+            raise ValueError("series64 must hold the batch's snapshots: same grid, number "
+                             "of snapshots and time periodicity")
         if sample_stride < 1:
             raise ValueError("sample_stride must be >= 1")
         K = 2 * self.series.grid.dim

@@ -383,3 +383,13 @@ def test_judge_hold_ab2_windows_readvect_to_the_fp64_bits(bf16_and_fp64):
                        first_snapshot=first, snapshot_dt=DT)
         torch.testing.assert_close(run.ftle, f, rtol=0, atol=0)
         torch.testing.assert_close(run.positions, pt, rtol=0, atol=0)
+
+
+def test_judge_rejects_a_judge_series_of_other_snapshots(bf16_and_fp64):
+    sbf, s64 = bf16_and_fp64
+    batch, _ = _batch(sbf, _windows(np.random.default_rng(16), count=2))
+    periodic = SnapshotSeries(s64.grid, torch.zeros((S, 2, s64.grid.nodes), dtype=torch.float64,
+                                                    device="cuda"),
+                              precision="fp64", periodic_time=True)
+    with pytest.raises(ValueError, match="time periodicity"):
+        batch.run_judged(periodic)
